@@ -1,0 +1,320 @@
+// war_batched.cu — the persistent refill kernel (war_enumerate).
+//
+// The reference gives every thread 256 consecutive deals and plays them one after another, so a warp
+// runs each deal slot as long as its longest game (gpu/war_gpu.py:149-165).  Here every lane keeps
+// G games in flight and steps all of them every iteration; a lane whose game is decided records it and
+// loads its next position at once, so uneven game lengths do not idle the warp.  The grid is
+// persistent (SMs x resident blocks) and lanes pull work units from one global atomic counter.
+//
+// Enumeration inside a unit: a unit is the block of j! consecutive lexicographic ranks that share a
+// prefix, i.e. every order of the last j positions.  The counts are sums and maxima over that SET, so
+// the lane walks it in Heap's order (one transposition per step, the counter packed in nibbles)
+// instead of lexicographic order; the set is the same.  Deals are held in a split layout: deck
+// position p lives in slot (p>>1) + 8*(p&1), so player 1's cards are the low 32 bits and player 2's
+// the high 32 bits and dealing is two ORs (war_cycles, gpu/war_gpu.py:98-107).
+//
+// Cycle detection is Brent (gpu/war_gpu.py:77-96) with the tortoise saved at steps W, 3W, 7W, ...;
+// W = 1 is the reference's schedule.  With W >= lam the first window compares every state with the
+// starting position itself, so a canonical start that lies on its cycle is recognised at no cost,
+// and the distinct-cycle walk of gpu/war_gpu.py:224-234 runs only for those few positions.
+#include "war_kernels.cuh"
+
+namespace war {
+
+struct Enum {
+    u64 P;       // current order: split layout (deals) or packed q (canon)
+    u32 ctr;     // Heap counter, digit i in nibble i
+    u32 full;    // counter value of the unit's last order
+    u32 base;    // first permuted position, M - j
+    u32 k, k0, k1;
+    bool live;   // P (and k) name the next unplayed position
+};
+
+template <bool CANON>
+__device__ __forceinline__ u32 pos_shift(u32 p) {
+    return CANON ? 4u * p : 4u * ((p >> 1) + ((p & 1u) << 3));
+}
+
+__device__ __forceinline__ u32 heap_full(u32 j) {
+    u32 f = 0;
+    for (u32 i = 1; i < j; i++) f |= i << (4u * i);
+    return f;
+}
+
+template <bool CANON>
+__device__ __forceinline__ bool fetch_unit(Enum& E, const BatchArgs& a, DevAcc* acc) {
+    u64 u = atomicAdd(&acc->work_next, 1ull);
+    if (u >= a.n_units) return false;
+    u64 r;
+    u32 j, k0, k1;
+    if (u < a.main_count) {
+        j = (u32)a.m; r = (a.main_base + u) * a.fact[a.m]; k0 = 0; k1 = (u32)a.n - 1u;
+    } else {
+        const Unit U = a.units[u - a.main_count];
+        r = U.r; j = U.j; k0 = U.k0; k1 = U.k1;
+    }
+    const int M = CANON ? a.n - 1 : a.n;
+    u64 p = unrank_packed(r, M, a.fact);
+    if (!CANON) p = compact_even_nibbles(p) | (compact_even_nibbles(p >> 4) << 32);
+    E.P = p;
+    E.ctr = 0;
+    E.full = heap_full(j);
+    E.base = (u32)M - j;
+    E.k0 = k0; E.k1 = k1; E.k = k0;
+    E.live = true;
+    return true;
+}
+
+// Heap's algorithm, one output: the lowest digit i with ctr[i] < i increments, the digits below it
+// reset to 0, and position i swaps with position 0 (i even) or ctr[i] (i odd).  False after the last.
+template <bool CANON>
+__device__ __forceinline__ bool heap_step(Enum& E) {
+    u32 x = E.ctr ^ E.full;
+    if (x == 0u) return false;
+    u32 i = (u32)(__ffs((int)x) - 1) >> 2;
+    u32 ci = (E.ctr >> (4u * i)) & 15u;
+    u32 o = (i & 1u) ? ci : 0u;
+    E.P = swap_nibbles(E.P, pos_shift<CANON>(E.base + i), pos_shift<CANON>(E.base + o));
+    E.ctr = ((E.ctr >> (4u * i)) + 1u) << (4u * i);
+    return true;
+}
+
+struct DealConst { u64 s1, s2; u32 q0, pat32; };
+
+// Next deal of the lane (deals mode); false when the lane has no work left.
+__device__ __forceinline__ bool next_deal(Enum& E, const BatchArgs& a, DevAcc* acc, const DealConst& c, u64& w1,
+                                          u64& w2, u32& q) {
+    for (;;) {
+        if (!E.live && !fetch_unit<false>(E, a, acc)) return false;
+        u64 D = E.P;
+        E.live = heap_step<false>(E);
+        if (a.half) {   // gpu/war_gpu.py:151-154: card n-1 dealt to player 1
+            u32 x = (u32)D ^ c.pat32;
+            if (((x - 0x11111111u) & ~x & 0x88888888u) == 0u) continue;
+        }
+        w1 = (D & 0xFFFFFFFFull) | c.s1;
+        w2 = (D >> 32) | c.s2;
+        q = c.q0;
+        return true;
+    }
+}
+
+// Next canonical position of the lane.
+__device__ __forceinline__ bool next_canon(Enum& E, const BatchArgs& a, DevAcc* acc, u64& w1, u64& w2, u32& q) {
+    if (!E.live && !fetch_unit<true>(E, a, acc)) return false;
+    canon_position(E.P, (u32)a.n, E.k, w1, w2, q);
+    if (++E.k == E.k1) {
+        E.k = E.k0;
+        E.live = heap_step<true>(E);
+    }
+    return true;
+}
+
+// One game slot.  EXTRA keeps the start position and the sample bit (distinct walk, sample);
+// SHAPE keeps the run tracker of the current tortoise window.
+template <bool EXTRA, bool SHAPE>
+struct Game {
+    u64 w1, w2, t1, t2;
+    u32 q, rounds, next;
+    bool active;
+    // EXTRA
+    u64 s1, s2; u32 sq; bool sampled;
+    // SHAPE: run tracker since the last tortoise save
+    u32 cur, first_run; bool first, prev, started, ok;
+};
+
+template <int RULE, int G, bool CANON, bool SHAPE, bool EXTRA>
+__global__ void __launch_bounds__(G == 1 ? 1024 : 512) batched_kernel(const __grid_constant__ BatchArgs a,
+                                                                     DevAcc* __restrict__ acc) {
+    extern __shared__ u32 sh[];
+    u32* shh = sh;
+    u32* she = sh + a.hbins;
+    for (int b = threadIdx.x; b < a.hbins + WAR_EBINS; b += blockDim.x) sh[b] = 0;
+    __syncthreads();
+
+    const u32 n = (u32)a.n, n4 = 4u * n, k4m4 = 4u * (n - 1u), W = (u32)a.W;
+    const u32 hb1 = a.hbins > 0 ? (u32)(a.hbins - 1) : 0u;
+    DealConst dc;
+    dc.s1 = sentinel_bit((n + 1u) / 2u);
+    dc.s2 = sentinel_bit(n / 2u);
+    dc.q0 = 4u * ((n + 1u) / 2u);
+    dc.pat32 = 0x11111111u * (n - 1u);
+
+    Enum E;
+    E.live = false;
+    Game<EXTRA, SHAPE> g[G];
+    u32 cyc = 0, done = 0, maxfin = 0, capped = 0;
+    u64 turns = 0;
+    u32 sc = 0, scy = 0, slam = 0, slen = 0, smax = 0, oncyc = 0, dmin = 0, nonstd = 0, unchk = 0;
+
+    auto start_game = [&](Game<EXTRA, SHAPE>& x) {
+        x.active = CANON ? next_canon(E, a, acc, x.w1, x.w2, x.q) : next_deal(E, a, acc, dc, x.w1, x.w2, x.q);
+        if (!x.active) { x.w1 = 1ull; x.w2 = 1ull; x.q = 0u; }   // retired slot: two empty piles, stepped harmlessly
+        x.t1 = x.w1; x.t2 = x.w2; x.rounds = 0; x.next = W;
+        if (EXTRA) {
+            x.s1 = x.w1; x.s2 = x.w2; x.sq = x.q;
+            x.sampled = a.sample && x.active && war_pick(a.seed, a.thr, x.w1, x.w2);
+        }
+        if (SHAPE) x.cur = 0;
+    };
+
+#pragma unroll
+    for (int i = 0; i < G; i++) start_game(g[i]);
+
+    for (;;) {
+        bool fin[G];
+        bool anyfin = false;
+#pragma unroll
+        for (int i = 0; i < G; i++) {
+            Game<EXTRA, SHAPE>& x = g[i];
+            bool p1 = war_turn<RULE>(x.w1, x.w2, x.q, k4m4);
+            x.rounds++;
+            bool cy = (x.w1 == x.t1) & (x.w2 == x.t2);
+            bool en = (x.q == 0u) | (x.q == n4);
+            if (SHAPE) {
+                if (x.cur == 0u) { x.first = p1; x.prev = p1; x.cur = 1u; x.first_run = 0u; x.started = false; x.ok = true; }
+                else if (p1 == x.prev) x.cur++;
+                else {
+                    if (!x.started) { x.first_run = x.cur; x.started = true; }
+                    else x.ok = x.ok && (x.cur == (u32)a.blk);
+                    x.cur = 1u; x.prev = p1;
+                }
+            }
+            if (x.rounds == x.next && !cy) {
+                if (x.next > WAR_TURN_CAP) {
+                    if (x.active) capped++;
+                    x.active = false;
+                } else {
+                    x.t1 = x.w1; x.t2 = x.w2; x.next = 2u * x.next + W;
+                    if (SHAPE) x.cur = 0u;
+                }
+            }
+            fin[i] = (cy | en) & x.active;
+            anyfin |= fin[i];
+        }
+        if (__any_sync(WAR_FULL_MASK, anyfin)) {
+#pragma unroll
+            for (int i = 0; i < G; i++) {
+                Game<EXTRA, SHAPE>& x = g[i];
+                if (fin[i]) {
+                    const bool cy = (x.w1 == x.t1) & (x.w2 == x.t2);
+                    done++;
+                    turns += x.rounds;
+                    const u32 lam = x.rounds - ((x.next - W) >> 1);
+                    if (cy) {
+                        cyc++;
+                        if (a.hbins) atomicAdd(&shh[lam < hb1 ? lam : hb1], 1u);
+                        if (CANON && EXTRA && a.distinct) {
+                            const u32 tstep = (x.next - W) >> 1;
+                            bool on = (tstep == 0u) ? true
+                                    : (lam <= W ? false : on_cycle_walk<RULE>(x.s1, x.s2, x.sq, n, lam));
+                            if (on) {
+                                CycleWalk cw = cycle_walk<RULE>(x.s1, x.s2, x.sq, n, lam);
+                                oncyc++;
+                                if (cw.is_min) dmin++;
+                                if (a.dbins) {
+                                    u32 d = cw.sym ? cw.c1 : cw.c1 + cw.c2;
+                                    u32 db1 = (u32)(a.dbins - 1);
+                                    atomicAdd(&acc->dhist[d < db1 ? d : db1], 1ull);
+                                }
+                            }
+                        }
+                        if (SHAPE) {
+                            if (lam > 512u) unchk++;
+                            else {
+                                bool ok = x.started && x.ok;
+                                if (x.started) {
+                                    if (x.prev == x.first) ok = ok && (x.cur + x.first_run == (u32)a.blk);
+                                    else ok = ok && (x.cur == (u32)a.blk) && (x.first_run == (u32)a.blk);
+                                }
+                                if (!ok) nonstd++;
+                            }
+                        }
+                    } else {
+                        if (x.rounds > maxfin) maxfin = x.rounds;
+                        atomicAdd(&she[x.rounds < WAR_EBINS - 1 ? x.rounds : WAR_EBINS - 1], 1u);
+                    }
+                    if (EXTRA && x.sampled) {
+                        sc++;
+                        if (cy) { scy++; slam += lam; }
+                        else { slen += x.rounds; if (x.rounds > smax) smax = x.rounds; }
+                    }
+                    start_game(x);
+                }
+            }
+            bool alive = false;
+#pragma unroll
+            for (int i = 0; i < G; i++) alive |= g[i].active;
+            if (!__any_sync(WAR_FULL_MASK, alive)) break;
+        }
+    }
+
+    u64 v_cyc = warp_sum(cyc), v_done = warp_sum(done), v_turns = warp_sum(turns), v_max = warp_max(maxfin);
+    u64 v_cap = warp_sum(capped);
+    if ((threadIdx.x & 31) == 0) {
+        if (v_cyc) atomicAdd(&acc->cyc, v_cyc);
+        if (v_done) atomicAdd(&acc->done, v_done);
+        if (v_turns) atomicAdd(&acc->turns, v_turns);
+        if (v_max) atomicMax(&acc->maxfin, v_max);
+        if (v_cap) atomicAdd(&acc->status, v_cap);
+    }
+    if (EXTRA) {
+        u64 v_sc = warp_sum(sc), v_scy = warp_sum(scy), v_slam = warp_sum(slam), v_slen = warp_sum(slen);
+        u64 v_smax = warp_max(smax), v_on = warp_sum(oncyc), v_dmin = warp_sum(dmin);
+        if ((threadIdx.x & 31) == 0) {
+            if (v_sc) {
+                atomicAdd(&acc->s_count, v_sc); atomicAdd(&acc->s_cyc, v_scy); atomicAdd(&acc->s_lamsum, v_slam);
+                atomicAdd(&acc->s_lensum, v_slen); atomicMax(&acc->s_maxfin, v_smax);
+            }
+            if (v_on) atomicAdd(&acc->oncycle, v_on);
+            if (v_dmin) atomicAdd(&acc->distinct_min, v_dmin);
+        }
+    }
+    if (SHAPE) {
+        u64 v_ns = warp_sum(nonstd), v_un = warp_sum(unchk);
+        if ((threadIdx.x & 31) == 0) {
+            if (v_ns) atomicAdd(&acc->shape_nonstd, v_ns);
+            if (v_un) atomicAdd(&acc->shape_unchecked, v_un);
+        }
+    }
+    __syncthreads();
+    flush_hist(shh, acc->hist, a.hbins);
+    flush_hist(she, acc->endhist, WAR_EBINS);
+}
+
+// ---- dispatch over the compiled variants ----------------------------------------------------------
+
+typedef void (*BatchedFn)(const BatchArgs, DevAcc*);
+
+template <int RULE, int G>
+static BatchedFn pick_g(int canon, int shape, int extra) {
+    if (!canon) return extra ? batched_kernel<RULE, G, false, false, true> : batched_kernel<RULE, G, false, false, false>;
+    if (shape) return extra ? batched_kernel<RULE, G, true, true, true> : batched_kernel<RULE, G, true, true, false>;
+    return extra ? batched_kernel<RULE, G, true, false, true> : batched_kernel<RULE, G, true, false, false>;
+}
+
+static BatchedFn pick(int canon, int rule, int shape, int extra, int games) {
+    if (rule) return games == 2 ? pick_g<1, 2>(canon, shape, extra) : pick_g<1, 1>(canon, shape, extra);
+    return games == 2 ? pick_g<0, 2>(canon, shape, extra) : pick_g<0, 1>(canon, shape, extra);
+}
+
+cudaError_t launch_batched(const BatchArgs& a, int canon, int rule, int shape, const BatchShape& bs, DevAcc* acc,
+                           cudaStream_t st) {
+    int extra = (a.distinct || a.sample) ? 1 : 0;
+    BatchedFn fn = pick(canon, rule, canon && shape, extra, bs.games);
+    size_t shmem = sizeof(u32) * (size_t)(a.hbins + WAR_EBINS);
+    fn<<<bs.blocks, bs.threads, shmem, st>>>(a, acc);
+    note_launch();
+    return cudaGetLastError();
+}
+
+int batched_max_blocks_per_sm(int canon, int rule, int shape, int distinct, int sample, int threads, int games,
+                              int hbins) {
+    BatchedFn fn = pick(canon, rule, canon && shape, (distinct || sample) ? 1 : 0, games);
+    int nb = 0;
+    size_t shmem = sizeof(u32) * (size_t)(hbins + WAR_EBINS);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, threads, shmem) != cudaSuccess) return 0;
+    return nb;
+}
+
+}  // namespace war

@@ -1,0 +1,54 @@
+// war_host.h — host-side state and helpers shared by the C ABI translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <mutex>
+#include <vector>
+#include "war_kernels.cuh"
+
+namespace war {
+
+struct Ctx {
+    static constexpr size_t UNIT_CAP = 1 << 16;
+    std::mutex mu;                  // serialises calls that launch work
+    bool ready = false;
+    int device = 0, sm_count = 0;
+    cudaStream_t own_stream = nullptr, user_stream = nullptr;
+    DevAcc* d_acc = nullptr;        // accumulators of the running job
+    DevAcc* h_acc = nullptr;        // pinned mirror
+    Unit* d_units = nullptr;        // extra work units of the running job
+    ulonglong2* d_sample = nullptr; // Floyd sample buffer
+    size_t sample_cap = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+struct Plan {
+    int m = 0;
+    u64 main_base = 0, main_count = 0;
+    u64 games_per_order = 1;
+    std::vector<Unit> extra;
+};
+
+struct Tune {
+    int threads, blocks_per_sm, games, block_m, window;
+};
+
+Ctx& ctx();
+int ensure_ready();
+cudaStream_t cur_stream();
+int fail(int code, const char* fmt, ...);
+int cuda_fail(cudaError_t e, const char* what);
+u64 fact(int i);
+u64 space_size(int n, int mode);
+int check_job(const war_job* j);
+void make_plan(const war_job* job, int m, Plan& p);
+void merge_acc(const DevAcc& h, war_result* r, int hbins, int dbins);
+void fill_fact(u64* f);
+int resolve_tune(const war_job* job, const war_tune* in, Tune& t);
+int floyd_sample_run(const war_job* job, war_result* out);
+
+cudaError_t launch_sample_scan(const FloydArgs& a, int threads, u64 nthreads, ulonglong2* buf, u64 cap, DevAcc* acc,
+                               cudaStream_t st);
+cudaError_t launch_floyd_play(const ulonglong2* buf, u64 cap, int n, int rule, int blocks, int threads, DevAcc* acc,
+                              cudaStream_t st);
+
+}  // namespace war
