@@ -161,7 +161,15 @@ __global__ void __launch_bounds__(G == 1 ? 1024 : 512) batched_kernel(const __gr
 #pragma unroll
     for (int i = 0; i < G; i++) start_game(g[i]);
 
-    for (;;) {
+    // The warp leaves the loop once none of its lanes holds an active game.  That test runs whenever a
+    // lane's set of active games can change (a game decided or abandoned at the cap), and once here for
+    // warps that got no work at all.
+    bool alive0 = false;
+#pragma unroll
+    for (int i = 0; i < G; i++) alive0 |= g[i].active;
+    bool running = __any_sync(WAR_FULL_MASK, alive0);
+
+    while (running) {
         bool fin[G];
         bool anyfin = false;
 #pragma unroll
@@ -180,9 +188,9 @@ __global__ void __launch_bounds__(G == 1 ? 1024 : 512) batched_kernel(const __gr
                     x.cur = 1u; x.prev = p1;
                 }
             }
-            if (x.rounds == x.next && !cy) {
+            if (x.rounds == x.next && !(cy | en)) {   // a decided game keeps its tortoise (the record reads it)
                 if (x.next > WAR_TURN_CAP) {
-                    if (x.active) capped++;
+                    if (x.active) { capped++; anyfin = true; }
                     x.active = false;
                 } else {
                     x.t1 = x.w1; x.t2 = x.w2; x.next = 2u * x.next + W;
@@ -245,7 +253,7 @@ __global__ void __launch_bounds__(G == 1 ? 1024 : 512) batched_kernel(const __gr
             bool alive = false;
 #pragma unroll
             for (int i = 0; i < G; i++) alive |= g[i].active;
-            if (!__any_sync(WAR_FULL_MASK, alive)) break;
+            running = __any_sync(WAR_FULL_MASK, alive);
         }
     }
 

@@ -86,6 +86,10 @@ __global__ void __launch_bounds__(256) floyd_kernel(const ulonglong2* __restrict
     refill();
     for (;;) {
         bool fin = false, cyc = false;
+        if (active && (steps > WAR_TURN_CAP || lam > WAR_TURN_CAP)) {   // never expected: abandon and flag
+            atomicAdd(&acc->status, 1ull);
+            refill();
+        }
         if (active) {
             if (phase == 0u) {
                 war_turn<RULE>(h1, h2, hq, k4m4); steps++;
