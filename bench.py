@@ -38,6 +38,9 @@ WORKLOADS = {
     "canon14": dict(n=14, mode=1, hbins=256, dbins=4096, flags=2 | 8, sample_ppm=10000, seed=14,
                     label="n=14 canonical positions, --distinct, --hist 256, 1% Floyd sample"),
     "deals11": dict(n=11, mode=0, hbins=256, flags=0, label="n=11 all deals"),
+    # a 2e8-deal slice from the middle of the n = 13 space (profiling size)
+    "deals13slice": dict(n=13, mode=0, hbins=256, flags=0, lo=3013510400, hi=3213510400,
+                         label="n=13 deals, ranks [3013510400, 3213510400)"),
 }
 
 
@@ -155,21 +158,19 @@ def reference_arm(args, rank, ws):
         assert deals == total
         sample, kind, units = "full run of cpu/war.cpp %d 0 (%d deals)" % (n, total), "reference", total
     else:
-        # strided sample of the rank space: 64 slices spread evenly, ~20 s of work in all
-        per_step_units = max(64, int(2.0e6 * cores / (110 if mode == 0 else 40)))
-        slice_len = max(1, per_step_units // 64)
-        for s in range(args.warmup + args.steps):
-            t0 = time.time()
-            for i in range(64):
-                lo = (total // 64) * i + (s * 7919 % max(1, total // 64 - slice_len))
-                job = oracle.make_job(n, mode, 0, w["flags"] & ~8, lo, min(total, lo + slice_len), hbins=w["hbins"],
-                                      dbins=w.get("dbins", 0))
-                oracle.enumerate_job(job, cores)
-            if s >= args.warmup:
-                times.append(time.time() - t0)
-        units = slice_len * 64
-        sample, kind = "64 strided slices of %d ranks (%d ranks per step) of the %s space" % (
-            slice_len, units, "canonical-position" if mode else "deal"), "port"
+        # bounded strided samples of the same rank space, ~150 s in all
+        per_step = 150.0 / max(1, args.steps + 1)
+        _oracle_sample_rate(w, min(per_step, 10.0), cores)           # warm-up
+        done_units = 0
+        for s in range(args.steps):
+            v, slice_len = _oracle_sample_rate(w, per_step, cores, seed=s + 1)
+            times.append(slice_len * 64 / v)
+            done_units += slice_len * 64
+        units = done_units / len(times)
+        sample, kind = ("64 strided slices of %d ranks of the %s space per step (oracle restatement of the "
+                        "reference algorithm; a full cpu/war.cpp run is estimated at %s s here)" % (
+                            slice_len, "canonical-position" if mode else "deal",
+                            "%.0f" % est if est else "n/a"), "port")
     t = sum(times) / len(times)
     v = units / t
     line.update({"value": v, "ms_per_step": t * 1e3,
@@ -179,24 +180,39 @@ def reference_arm(args, rank, ws):
     print(json.dumps(line), flush=True)
 
 
-def cpu_baseline(w, cores_budget_s=12.0):
-    """The oracle's restatement of the reference algorithm on a bounded strided sample (all host threads)."""
+def _oracle_sample_rate(w, target_s, cores, seed=0):
+    """Times the oracle's restatement of the reference algorithm on a strided sample of the workload's
+    rank space (64 slices spread evenly), sized by a short probe to take about target_s seconds."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     n, mode = w["n"], w["mode"]
-    cores = os.cpu_count() or 1
     total = space(n, mode)
-    slice_len = max(1, int(1.5e6 * cores / (110 if mode == 0 else 40)) // 64)
-    t0 = time.time()
-    for i in range(64):
-        lo = (total // 64) * i
-        job = oracle.make_job(n, mode, 0, w["flags"] & ~8, lo, min(total, lo + slice_len), hbins=w["hbins"],
-                              dbins=w.get("dbins", 0))
-        oracle.enumerate_job(job, cores)
-    dt = time.time() - t0
-    return {"value": slice_len * 64 / dt, "unit": "positions/s" if mode else "deals/s", "cores": cores, "kind": "port",
-            "sample": "64 strided slices of %d ranks of the %s space (oracle restatement of cpu/war.cpp's "
-                      "algorithm, OpenMP)" % (slice_len, "canonical-position" if mode else "deal")}
+
+    def run(slice_len):
+        t0 = time.time()
+        for i in range(64):
+            lo = (total // 64) * i + (seed * 7919) % max(1, total // 64 - slice_len)
+            job = oracle.make_job(n, mode, 0, w["flags"] & ~8, lo, min(total, lo + slice_len), hbins=w["hbins"],
+                                  dbins=w.get("dbins", 0))
+            oracle.enumerate_job(job, cores)
+        return time.time() - t0
+
+    probe = 4096
+    dt = run(probe)
+    slice_len = max(probe, int(probe * target_s / max(dt, 1e-3)))
+    dt = run(slice_len)
+    return slice_len * 64 / dt, slice_len
+
+
+def cpu_baseline(w, target_s=12.0):
+    """The oracle's restatement of the reference algorithm on a bounded strided sample (all host threads)."""
+    cores = os.cpu_count() or 1
+    v, slice_len = _oracle_sample_rate(w, target_s, cores)
+    mode = w["mode"]
+    return {"value": v, "unit": "positions/s" if mode else "deals/s", "cores": cores, "kind": "port",
+            "sample": "64 strided slices of %d ranks of the %s space, oracle/war_oracle.c (restatement of "
+                      "cpu/war.cpp's algorithm, OpenMP on all host threads), ~%.0f s" % (
+                          slice_len, "canonical-position" if mode else "deal", target_s)}
 
 
 def main():
@@ -223,8 +239,9 @@ def main():
     import war_gpu
     w = WORKLOADS[args.workload]
     n, mode = w["n"], w["mode"]
-    total = space(n, mode)
-    lo, hi = total * rank // ws, total * (rank + 1) // ws
+    lo0, hi0 = w.get("lo", 0), w.get("hi", space(n, mode))
+    total = hi0 - lo0
+    lo, hi = lo0 + total * rank // ws, lo0 + total * (rank + 1) // ws
     job = warlib.make_job(n, mode, 0, w["flags"], lo, hi, hbins=w["hbins"], dbins=w.get("dbins", 0),
                           sample_ppm=w.get("sample_ppm", 0), seed=w.get("seed", 0))
     torch.cuda.set_device(local)
@@ -232,13 +249,15 @@ def main():
     warlib.set_stream(stream.cuda_stream)
     tune = war_gpu._tune_for(n, mode == 1, 0, w["flags"])
 
+    floyd_ms = []
+
     def step():
         r = warlib.enumerate_job(job, tune)
         if w["flags"] & 8:
             f = warlib.floyd_sample(job)
             assert (f.s_count, f.s_cyc, f.s_lamsum, f.s_lensum, f.s_maxfin) == \
                 (r.s_count, r.s_cyc, r.s_lamsum, r.s_lensum, r.s_maxfin), "Floyd sample disagrees with Brent"
-            r.kernel_ms += f.kernel_ms
+            floyd_ms.append(f.kernel_ms)
         return r
 
     for _ in range(args.warmup):
@@ -272,7 +291,7 @@ def main():
         m = torch.tensor([acc[2]], dtype=torch.int64, device="cuda")
         dist.all_reduce(m, op=dist.ReduceOp.MAX)
         acc = [int(t[0]), int(t[1]), int(m[0]), int(t[2]), int(t[3]), int(t[4])]
-    check = verify(w, acc, res if ws == 1 else None)
+    check = verify(w, acc, res if ws == 1 else None) if "lo" not in w else "slice (no recorded total)"
 
     # e2e through the public drop-in API (war_gpu.run), host buffers, copies inside the timed region
     e2e = None
@@ -282,7 +301,7 @@ def main():
         torch.cuda.synchronize()
         barrier(ws)
         t0 = time.perf_counter()
-        if ws == 1:
+        if ws == 1 and "lo" not in w:
             war_gpu.run(n, **kw)
         else:
             r2 = warlib.enumerate_job(job, tune)
@@ -309,6 +328,7 @@ def main():
             "turns_per_s": turns * ws / (ms_max * 1e-3 / args.steps),
             "turns_per_step": turns * ws,
             "kernel_ms": kernel_ms,
+            "floyd_check_ms": (sum(floyd_ms[-args.steps:]) / args.steps) if floyd_ms else None,
             "gpu_launches": launches,
             "roofline": {"bound": "int_issue", "achieved": achieved / 1e12, "peak": issue_peak / 1e12,
                          "unit": "Tops/s (INT32 thread-ops)", "frac": achieved / issue_peak,

@@ -112,18 +112,19 @@ __device__ __forceinline__ bool next_canon(Enum& E, const BatchArgs& a, DevAcc* 
 
 // One game slot.  EXTRA keeps the start position and the sample bit (distinct walk, sample);
 // SHAPE keeps the run tracker of the current tortoise window.
+enum { ST_ACTIVE = 0, ST_WAITING = 1, ST_RETIRED = 2 };
+
 template <bool EXTRA, bool SHAPE>
 struct Game {
     u64 w1, w2, t1, t2;
-    u32 q, rounds, next;
-    bool active;
+    u32 q, rounds, next, st;
     // EXTRA
     u64 s1, s2; u32 sq; bool sampled;
     // SHAPE: run tracker since the last tortoise save
     u32 cur, first_run; bool first, prev, started, ok;
 };
 
-template <int RULE, int G, bool CANON, bool SHAPE, bool EXTRA>
+template <int RULE, int G, bool CANON, bool SHAPE, bool EXTRA, int TV>
 __global__ void __launch_bounds__(G == 1 ? 1024 : 512) batched_kernel(const __grid_constant__ BatchArgs a,
                                                                      DevAcc* __restrict__ acc) {
     extern __shared__ u32 sh[];
@@ -133,6 +134,9 @@ __global__ void __launch_bounds__(G == 1 ? 1024 : 512) batched_kernel(const __gr
     __syncthreads();
 
     const u32 n = (u32)a.n, n4 = 4u * n, k4m4 = 4u * (n - 1u), W = (u32)a.W;
+    const TurnK K = a.tk;
+    // TV = 0: war_turn (q = 4*len1); TV = 1: war_turn_fma (q holds qq = 4*len1 - 2n)
+    const u32 qshift = TV ? 2u * n : 0u;
     const u32 hb1 = a.hbins > 0 ? (u32)(a.hbins - 1) : 0u;
     DealConst dc;
     dc.s1 = sentinel_bit((n + 1u) / 2u);
@@ -143,30 +147,44 @@ __global__ void __launch_bounds__(G == 1 ? 1024 : 512) batched_kernel(const __gr
     Enum E;
     E.live = false;
     Game<EXTRA, SHAPE> g[G];
-    u32 cyc = 0, done = 0, maxfin = 0, capped = 0;
-    u64 turns = 0;
+    // Per-lane totals.  A launch plays fewer than 2^32 games in all, so no lane's 32-bit turn total wraps.
+    u32 cyc = 0, done = 0, maxfin = 0, capped = 0, turns = 0;
     u32 sc = 0, scy = 0, slam = 0, slen = 0, smax = 0, oncyc = 0, dmin = 0, nonstd = 0, unchk = 0;
 
+    // Game slot states: ACTIVE (being played), WAITING (decided and recorded, frozen until the warp
+    // refills), RETIRED (no work left).  A frozen slot holds two empty words and q far out of range, so
+    // the turn step leaves it unchanged (the pushed pair shifts out, shl64 gives 0).
+    // A frozen slot can never signal: its low words differ from its tortoise's, its length offset is far
+    // from both ends, and its next checkpoint is never reached.
+    auto freeze = [&](Game<EXTRA, SHAPE>& x) {
+        x.w1 = 0ull; x.w2 = 0ull; x.q = 0x80000000u; x.t1 = 1ull; x.t2 = 1ull; x.next = 0xFFFFFFFFu;
+    };
     auto start_game = [&](Game<EXTRA, SHAPE>& x) {
-        x.active = CANON ? next_canon(E, a, acc, x.w1, x.w2, x.q) : next_deal(E, a, acc, dc, x.w1, x.w2, x.q);
-        if (!x.active) { x.w1 = 1ull; x.w2 = 1ull; x.q = 0u; }   // retired slot: two empty piles, stepped harmlessly
+        bool ok = CANON ? next_canon(E, a, acc, x.w1, x.w2, x.q) : next_deal(E, a, acc, dc, x.w1, x.w2, x.q);
+        x.st = ok ? ST_ACTIVE : ST_RETIRED;
+        done += ok ? 1u : 0u;
         x.t1 = x.w1; x.t2 = x.w2; x.rounds = 0; x.next = W;
         if (EXTRA) {
             x.s1 = x.w1; x.s2 = x.w2; x.sq = x.q;
-            x.sampled = a.sample && x.active && war_pick(a.seed, a.thr, x.w1, x.w2);
+            x.sampled = a.sample && ok && war_pick(a.seed, a.thr, x.w1, x.w2);
         }
         if (SHAPE) x.cur = 0;
+        x.q -= qshift;
+        if (!ok) freeze(x);
     };
 
 #pragma unroll
     for (int i = 0; i < G; i++) start_game(g[i]);
 
-    // The warp leaves the loop once none of its lanes holds an active game.  That test runs whenever a
-    // lane's set of active games can change (a game decided or abandoned at the cap), and once here for
-    // warps that got no work at all.
+    // The warp leaves the loop once none of its lanes holds an active or waiting game.  That test runs
+    // whenever a slot changes state (a game decided or abandoned at the cap), and once here for warps that
+    // got no work at all.  Decided games wait, frozen, until `defer` lanes of the warp are waiting (or
+    // none is playing); then all of them load their next position together, so the refill code runs
+    // with many lanes at once instead of one.
+    const int defer = a.defer > 0 ? a.defer : 1;
     bool alive0 = false;
 #pragma unroll
-    for (int i = 0; i < G; i++) alive0 |= g[i].active;
+    for (int i = 0; i < G; i++) alive0 |= g[i].st == ST_ACTIVE;
     bool running = __any_sync(WAR_FULL_MASK, alive0);
 
     while (running) {
@@ -175,10 +193,19 @@ __global__ void __launch_bounds__(G == 1 ? 1024 : 512) batched_kernel(const __gr
 #pragma unroll
         for (int i = 0; i < G; i++) {
             Game<EXTRA, SHAPE>& x = g[i];
-            bool p1 = war_turn<RULE>(x.w1, x.w2, x.q, k4m4);
-            x.rounds++;
-            bool cy = (x.w1 == x.t1) & (x.w2 == x.t2);
-            bool en = (x.q == 0u) | (x.q == n4);
+            bool p1, en;
+            if (TV == 1) {
+                p1 = war_turn_fma<RULE>(x.w1, x.w2, x.q, K);
+                x.rounds = x.rounds * K.one + K.one;
+                en = x.q * x.q == K.end2;
+            } else {
+                p1 = war_turn<RULE>(x.w1, x.w2, x.q, k4m4);
+                x.rounds++;
+                en = (x.q == 0u) | (x.q == n4);
+            }
+            // Cycle candidate: the low words of both piles equal the tortoise's.  Exact equality of the
+            // high words is checked when the game is recorded; a candidate that fails it plays on.
+            bool cy = ((u32)x.w1 == (u32)x.t1) & ((u32)x.w2 == (u32)x.t2);
             if (SHAPE) {
                 if (x.cur == 0u) { x.first = p1; x.prev = p1; x.cur = 1u; x.first_run = 0u; x.started = false; x.ok = true; }
                 else if (p1 == x.prev) x.cur++;
@@ -190,23 +217,33 @@ __global__ void __launch_bounds__(G == 1 ? 1024 : 512) batched_kernel(const __gr
             }
             if (x.rounds == x.next && !(cy | en)) {   // a decided game keeps its tortoise (the record reads it)
                 if (x.next > WAR_TURN_CAP) {
-                    if (x.active) { capped++; anyfin = true; }
-                    x.active = false;
+                    if (x.st == ST_ACTIVE) { capped++; x.st = ST_WAITING; freeze(x); anyfin = true; }
                 } else {
                     x.t1 = x.w1; x.t2 = x.w2; x.next = 2u * x.next + W;
                     if (SHAPE) x.cur = 0u;
                 }
             }
-            fin[i] = (cy | en) & x.active;
+            fin[i] = cy | en;
             anyfin |= fin[i];
         }
         if (__any_sync(WAR_FULL_MASK, anyfin)) {
 #pragma unroll
             for (int i = 0; i < G; i++) {
                 Game<EXTRA, SHAPE>& x = g[i];
-                if (fin[i]) {
+                bool rec = fin[i];
+                if (rec) {
+                    const bool en = TV ? (x.q * x.q == K.end2) : ((x.q == 0u) | (x.q == n4));
+                    if (!en && !((x.w1 == x.t1) & (x.w2 == x.t2))) {
+                        // low words matched by chance: play on, with the tortoise save this step skipped
+                        rec = false;
+                        if (x.rounds == x.next) {
+                            x.t1 = x.w1; x.t2 = x.w2; x.next = 2u * x.next + W;
+                            if (SHAPE) x.cur = 0u;
+                        }
+                    }
+                }
+                if (rec) {
                     const bool cy = (x.w1 == x.t1) & (x.w2 == x.t2);
-                    done++;
                     turns += x.rounds;
                     const u32 lam = x.rounds - ((x.next - W) >> 1);
                     if (cy) {
@@ -247,17 +284,30 @@ __global__ void __launch_bounds__(G == 1 ? 1024 : 512) batched_kernel(const __gr
                         if (cy) { scy++; slam += lam; }
                         else { slen += x.rounds; if (x.rounds > smax) smax = x.rounds; }
                     }
-                    start_game(x);
+                    x.st = ST_WAITING;
+                    freeze(x);
                 }
             }
-            bool alive = false;
+            bool waiting = false, playing = false;
 #pragma unroll
-            for (int i = 0; i < G; i++) alive |= g[i].active;
-            running = __any_sync(WAR_FULL_MASK, alive);
+            for (int i = 0; i < G; i++) { waiting |= g[i].st == ST_WAITING; playing |= g[i].st == ST_ACTIVE; }
+            const u32 wb = __ballot_sync(WAR_FULL_MASK, waiting);
+            const u32 pb = __ballot_sync(WAR_FULL_MASK, playing);
+            if (__popc(wb) >= defer || pb == 0u) {
+                if (waiting) {
+#pragma unroll
+                    for (int i = 0; i < G; i++)
+                        if (g[i].st == ST_WAITING) start_game(g[i]);
+                }
+                playing = false;
+#pragma unroll
+                for (int i = 0; i < G; i++) playing |= g[i].st == ST_ACTIVE;
+                running = __any_sync(WAR_FULL_MASK, playing);
+            }
         }
     }
 
-    u64 v_cyc = warp_sum(cyc), v_done = warp_sum(done), v_turns = warp_sum(turns), v_max = warp_max(maxfin);
+    u64 v_cyc = warp_sum(cyc), v_done = warp_sum(done), v_turns = warp_sum((u64)turns), v_max = warp_max(maxfin);
     u64 v_cap = warp_sum(capped);
     if ((threadIdx.x & 31) == 0) {
         if (v_cyc) atomicAdd(&acc->cyc, v_cyc);
@@ -294,22 +344,27 @@ __global__ void __launch_bounds__(G == 1 ? 1024 : 512) batched_kernel(const __gr
 
 typedef void (*BatchedFn)(const BatchArgs, DevAcc*);
 
-template <int RULE, int G>
+template <int RULE, int G, int TV>
 static BatchedFn pick_g(int canon, int shape, int extra) {
-    if (!canon) return extra ? batched_kernel<RULE, G, false, false, true> : batched_kernel<RULE, G, false, false, false>;
-    if (shape) return extra ? batched_kernel<RULE, G, true, true, true> : batched_kernel<RULE, G, true, true, false>;
-    return extra ? batched_kernel<RULE, G, true, false, true> : batched_kernel<RULE, G, true, false, false>;
+    if (!canon) return extra ? batched_kernel<RULE, G, false, false, true, TV> : batched_kernel<RULE, G, false, false, false, TV>;
+    if (shape) return extra ? batched_kernel<RULE, G, true, true, true, TV> : batched_kernel<RULE, G, true, true, false, TV>;
+    return extra ? batched_kernel<RULE, G, true, false, true, TV> : batched_kernel<RULE, G, true, false, false, TV>;
 }
 
-static BatchedFn pick(int canon, int rule, int shape, int extra, int games) {
-    if (rule) return games == 2 ? pick_g<1, 2>(canon, shape, extra) : pick_g<1, 1>(canon, shape, extra);
-    return games == 2 ? pick_g<0, 2>(canon, shape, extra) : pick_g<0, 1>(canon, shape, extra);
+template <int TV>
+static BatchedFn pick_tv(int canon, int rule, int shape, int extra, int games) {
+    if (rule) return games == 2 ? pick_g<1, 2, TV>(canon, shape, extra) : pick_g<1, 1, TV>(canon, shape, extra);
+    return games == 2 ? pick_g<0, 2, TV>(canon, shape, extra) : pick_g<0, 1, TV>(canon, shape, extra);
+}
+
+static BatchedFn pick(int canon, int rule, int shape, int extra, int games, int variant) {
+    return variant == 1 ? pick_tv<1>(canon, rule, shape, extra, games) : pick_tv<0>(canon, rule, shape, extra, games);
 }
 
 cudaError_t launch_batched(const BatchArgs& a, int canon, int rule, int shape, const BatchShape& bs, DevAcc* acc,
                            cudaStream_t st) {
     int extra = (a.distinct || a.sample) ? 1 : 0;
-    BatchedFn fn = pick(canon, rule, canon && shape, extra, bs.games);
+    BatchedFn fn = pick(canon, rule, canon && shape, extra, bs.games, bs.variant);
     size_t shmem = sizeof(u32) * (size_t)(a.hbins + WAR_EBINS);
     fn<<<bs.blocks, bs.threads, shmem, st>>>(a, acc);
     note_launch();
@@ -317,8 +372,8 @@ cudaError_t launch_batched(const BatchArgs& a, int canon, int rule, int shape, c
 }
 
 int batched_max_blocks_per_sm(int canon, int rule, int shape, int distinct, int sample, int threads, int games,
-                              int hbins) {
-    BatchedFn fn = pick(canon, rule, canon && shape, (distinct || sample) ? 1 : 0, games);
+                              int hbins, int variant) {
+    BatchedFn fn = pick(canon, rule, canon && shape, (distinct || sample) ? 1 : 0, games, variant);
     int nb = 0;
     size_t shmem = sizeof(u32) * (size_t)(hbins + WAR_EBINS);
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, threads, shmem) != cudaSuccess) return 0;

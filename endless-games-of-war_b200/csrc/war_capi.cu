@@ -197,18 +197,22 @@ int resolve_tune(const war_job* job, const war_tune* in, Tune& t) {
     t.threads = (in && in->threads) ? in->threads : 256;
     t.games = (in && in->games) ? in->games : 1;
     t.block_m = (in && in->block_m) ? in->block_m : (canon ? 5 : 6);
-    t.window = (in && in->window) ? in->window : (canon ? 128 : 1);
+    t.window = (in && in->window) ? in->window : (canon ? 128 : 32);
+    t.defer = (in && in->defer) ? in->defer : 1;
+    t.variant = in ? in->variant : 0;
     if (t.threads < 64 || t.threads > 1024 || (t.threads & 31)) return fail(WAR_EINVAL, "tune.threads=%d", t.threads);
     if (t.games != 1 && t.games != 2) return fail(WAR_EINVAL, "tune.games=%d (1 or 2)", t.games);
     if (t.block_m < 1 || t.block_m > 8) return fail(WAR_EINVAL, "tune.block_m=%d (1..8)", t.block_m);
     if (t.window < 1 || t.window > (1 << 16) || (t.window & (t.window - 1))) return fail(WAR_EINVAL, "tune.window=%d", t.window);
+    if (t.defer < 1 || t.defer > 32) return fail(WAR_EINVAL, "tune.defer=%d (1..32)", t.defer);
+    if (t.variant != 0 && t.variant != 1) return fail(WAR_EINVAL, "tune.variant=%d (0 or 1)", t.variant);
     const int M = canon ? job->n - 1 : job->n;
     if (t.block_m > M) t.block_m = M > 0 ? M : 1;
     int st = ensure_ready();
     if (st) return st;
     int maxb = batched_max_blocks_per_sm(canon, job->rule, (job->flags & WAR_F_SHAPE) != 0,
                                          (job->flags & WAR_F_DISTINCT) != 0, (job->flags & WAR_F_SAMPLE) != 0,
-                                         t.threads, t.games, job->hbins);
+                                         t.threads, t.games, job->hbins, t.variant);
     if (maxb < 1) return fail(WAR_EINVAL, "launch shape threads=%d games=%d does not fit an SM", t.threads, t.games);
     t.blocks_per_sm = (in && in->blocks_per_sm) ? std::min(in->blocks_per_sm, maxb) : maxb;
     return WAR_OK;
@@ -482,7 +486,9 @@ int war_enumerate(const war_job* job, const war_tune* tune, war_result* out) {
     memset(&a, 0, sizeof a);
     fill_fact(a.fact);
     a.n = job->n; a.m = t.block_m; a.hbins = job->hbins; a.dbins = job->dbins;
-    a.blk = out->blk; a.W = t.window;
+    a.blk = out->blk; a.W = t.window; a.defer = t.defer;
+    a.tk.k16 = 16u; a.tk.km16 = (u32)-16; a.tk.k2p28 = 1u << 28; a.tk.k4 = 4u; a.tk.one = 1u;
+    a.tk.c0 = 2 * job->n - 4; a.tk.end2 = (u32)(4 * job->n * job->n);
     a.half = (job->flags & WAR_F_HALF) ? 1 : 0;
     a.sample = (job->flags & WAR_F_SAMPLE) ? 1 : 0;
     a.distinct = (job->flags & WAR_F_DISTINCT) && job->mode == WAR_CANON ? 1 : 0;
@@ -493,7 +499,7 @@ int war_enumerate(const war_job* job, const war_tune* tune, war_result* out) {
     const u64 per_unit = fact(t.block_m) * p.games_per_order;
     const u64 max_units = std::max<u64>(1, ((1ull << 32) - (1ull << 24)) / per_unit);
     BatchShape bs;
-    bs.threads = t.threads; bs.games = t.games; bs.blocks = t.blocks_per_sm * c.sm_count;
+    bs.threads = t.threads; bs.games = t.games; bs.blocks = t.blocks_per_sm * c.sm_count; bs.variant = t.variant;
     const int shape = (job->flags & WAR_F_SHAPE) && job->mode == WAR_CANON ? 1 : 0;
     u64 done_main = 0;
     bool extras_done = p.extra.empty();

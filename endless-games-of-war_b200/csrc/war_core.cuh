@@ -45,6 +45,52 @@ __device__ __forceinline__ bool war_turn(u64& w1, u64& w2, u32& q, u32 k4m4) {
     return p1;
 }
 
+// Constants of war_turn_fma, passed in from kernel arguments so that the compiler keeps them as
+// multiplier operands instead of folding them into shifts.
+struct TurnK {
+    u32 k16;    // 16
+    u32 km16;   // -16
+    u32 k2p28;  // 2^28
+    u32 k4;     // 4
+    u32 one;    // 1
+    int c0;     // 2n - 4
+    u32 end2;   // (2n)^2
+};
+
+// The same turn as war_turn, written so that about half of its integer operations are multiply-adds
+// (the FMA pipe) rather than logic / shift operations (the ALU pipe, half rate on sm_100):
+//   pop:   lo' = funnel(lo, hi) >> 4, hi' = mulhi(hi, 2^28) = hi >> 4, card = lo - 16*lo' (mod 2^32)
+//   pair:  c1 + 16*c2 and c2 + 16*c1 by IMAD, one select
+//   push:  the winner's word gains (pair + 0xFF) << pos (the sentinel bit at pos becomes the pair and
+//          a new sentinel 8 bits up; the same bits as war_turn's XOR), added as w += x*b with b in {0,1}
+//          by mad.wide, so no select or mask is needed
+//   length: qq = 4*len1 - 2n, pos = s*qq + (2n-4) and qq += 4s with s = +1 (player 1 won) or -1;
+//          the game is over when qq*qq == (2n)^2.
+template <int RULE>
+__device__ __forceinline__ bool war_turn_fma(u64& w1, u64& w2, u32& qq, const TurnK& K) {
+    const u32 l1 = (u32)w1, h1 = (u32)(w1 >> 32), l2 = (u32)w2, h2 = (u32)(w2 >> 32);
+    const u32 nl1 = __funnelshift_r(l1, h1, 4), nl2 = __funnelshift_r(l2, h2, 4);
+    const u32 nh1 = __umulhi(h1, K.k2p28), nh2 = __umulhi(h2, K.k2p28);
+    const u32 c1 = l1 + nl1 * K.km16, c2 = l2 + nl2 * K.km16;
+    const bool p1 = c1 > c2;
+    const u32 pa = RULE ? c2 + c1 * K.k16 : c1 + c2 * K.k16;   // player 1 won
+    const u32 pb = RULE ? c1 + c2 * K.k16 : c2 + c1 * K.k16;   // player 2 won
+    const u32 term = (p1 ? pa : pb) + 0xFFu;
+    const int s = p1 ? 1 : -1;
+    const u32 pos = (u32)(s * (int)qq + K.c0);
+    const u64 x = shl64((u64)term, pos);
+    const u32 xl = (u32)x, xh = (u32)(x >> 32);
+    const u32 b1 = p1 ? 1u : 0u, b2 = K.one - b1;
+    u64 a1 = ((u64)nh1 << 32) | nl1, a2 = ((u64)nh2 << 32) | nl2;
+    a1 = (u64)xl * b1 + a1;
+    a2 = (u64)xl * b2 + a2;
+    const u32 a1h = (u32)(a1 >> 32) + xh * b1, a2h = (u32)(a2 >> 32) + xh * b2;
+    w1 = ((u64)a1h << 32) | (u32)a1;
+    w2 = ((u64)a2h << 32) | (u32)a2;
+    qq = qq + (u32)s * K.k4;
+    return p1;
+}
+
 // The same turn with the rule chosen at run time (serving kernel, checks).
 __device__ __forceinline__ bool war_turn_rt(u64& w1, u64& w2, u32& q, u32 k4m4, int rule) {
     return rule ? war_turn<1>(w1, w2, q, k4m4) : war_turn<0>(w1, w2, q, k4m4);

@@ -29,7 +29,7 @@ struct Plan {
 };
 
 struct Tune {
-    int threads, blocks_per_sm, games, block_m, window;
+    int threads, blocks_per_sm, games, block_m, window, defer, variant;
 };
 
 Ctx& ctx();

@@ -34,7 +34,8 @@ struct BatchArgs {
     u64 n_units;       // main_count + extra units
     const Unit* units; // extra units, handed out after the main ones
     u64 seed, thr;
-    int n, m, hbins, dbins, blk, W, half, sample, distinct;
+    TurnK tk;          // constants of war_turn_fma
+    int n, m, hbins, dbins, blk, W, half, sample, distinct, defer;
 };
 
 struct CycleWalk { u32 c1, c2; bool sym, on, is_min; };
@@ -120,11 +121,11 @@ void note_launch();
 cudaError_t launch_plain(const PlainArgs& a, int canon, int rule, int threads, u64 nthreads, DevAcc* acc,
                          cudaStream_t st);
 
-struct BatchShape { int threads, blocks, games; };
+struct BatchShape { int threads, blocks, games, variant; };
 cudaError_t launch_batched(const BatchArgs& a, int canon, int rule, int shape, const BatchShape& bs, DevAcc* acc,
                            cudaStream_t st);
 int batched_max_blocks_per_sm(int canon, int rule, int shape, int distinct, int sample, int threads, int games,
-                              int hbins);
+                              int hbins, int variant);
 
 struct FloydArgs {
     u64 fact[17];
