@@ -154,10 +154,12 @@ __global__ void __launch_bounds__(G == 1 ? 1024 : 512) batched_kernel(const __gr
     // Game slot states: ACTIVE (being played), WAITING (decided and recorded, frozen until the warp
     // refills), RETIRED (no work left).  A frozen slot holds two empty words and q far out of range, so
     // the turn step leaves it unchanged (the pushed pair shifts out, shl64 gives 0).
-    // A frozen slot can never signal: its low words differ from its tortoise's, its length offset is far
-    // from both ends, and its next checkpoint is never reached.
+    // A frozen slot can never signal: its low words differ from its tortoise's, its next checkpoint is
+    // never reached, and its length offset is odd and far from both ends.  Every turn moves the offset by
+    // 4, so it stays odd: never 0 or 4n, and its square (multiply-add form) is odd, never (2n)^2.  With
+    // both words empty the pushed pair lands beyond bit 63 and the words stay 0.
     auto freeze = [&](Game<EXTRA, SHAPE>& x) {
-        x.w1 = 0ull; x.w2 = 0ull; x.q = 0x80000000u; x.t1 = 1ull; x.t2 = 1ull; x.next = 0xFFFFFFFFu;
+        x.w1 = 0ull; x.w2 = 0ull; x.q = 0x80000001u; x.t1 = 1ull; x.t2 = 1ull; x.next = 0xFFFFFFFFu;
     };
     auto start_game = [&](Game<EXTRA, SHAPE>& x) {
         bool ok = CANON ? next_canon(E, a, acc, x.w1, x.w2, x.q) : next_deal(E, a, acc, dc, x.w1, x.w2, x.q);
