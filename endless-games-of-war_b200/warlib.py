@@ -86,6 +86,7 @@ SYMBOLS = {
     "war_enumerate_plain": (ctypes.c_int, [ctypes.POINTER(Job), ctypes.POINTER(Result)]),
     "war_enumerate": (ctypes.c_int, [ctypes.POINTER(Job), ctypes.POINTER(Tune), ctypes.POINTER(Result)]),
     "war_floyd_sample": (ctypes.c_int, [ctypes.POINTER(Job), ctypes.POINTER(Result)]),
+    "war_enumerate_noalloc": (ctypes.c_int, [ctypes.POINTER(Job), ctypes.POINTER(Tune), ctypes.POINTER(Result)]),
     "war_server_create": (ctypes.c_int, [ctypes.POINTER(ServerCfg), ctypes.POINTER(ctypes.c_void_p)]),
     "war_server_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Job), U64P]),
     "war_server_poll": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(Result), ctypes.POINTER(JobStatus)]),
@@ -153,6 +154,15 @@ def enumerate_job(job, tune=None):
     r = Result()
     check(lib().war_enumerate(ctypes.byref(job), ctypes.byref(tune) if tune is not None else None, ctypes.byref(r)),
           "war_enumerate")
+    return r
+
+
+def enumerate_noalloc(job, tune=None):
+    """war_enumerate_noalloc: the same enumeration with the library's static scratch instead of allocated
+    device memory, for callers that cannot allocate (see include/war.h)."""
+    r = Result()
+    check(lib().war_enumerate_noalloc(ctypes.byref(job), ctypes.byref(tune) if tune is not None else None,
+                                      ctypes.byref(r)), "war_enumerate_noalloc")
     return r
 
 

@@ -133,6 +133,18 @@ int war_enumerate_plain(const war_job* job, war_result* out);
  * with the next deal or position as soon as its game is decided.  tune may be NULL (defaults). */
 int war_enumerate(const war_job* job, const war_tune* tune, war_result* out);
 
+/* war_enumerate for callers that cannot allocate device memory: a host program whose own memory pool
+ * has reserved the GPU (a cudaMalloc would fail or fragment it), or code on a latency-bound path that
+ * cannot take cudaMalloc's implicit synchronisation.  No counterpart in the reference.  Same kernel,
+ * arguments and results as war_enumerate (kernel_ms is host wall time here), but its scratch (one job's
+ * accumulators and work counter, and at most 1024 extra work units; about 98 KB) lives in a static
+ * device array that every GPU loading the library holds until exit; jobs whose plan needs more extra
+ * units are refused with WAR_EINVAL.  The first call on each device looks up that array's address
+ * (cudaGetSymbolAddress) and should come before any stream capture.  It calls no cudaMalloc / cudaFree
+ * and creates no stream or event.  All calls share the array: each clears it before use, and calls
+ * whose work overlaps on the GPU race. */
+int war_enumerate_noalloc(const war_job* job, const war_tune* tune, war_result* out);
+
 /* Floyd cross-check (the second detector of gpu/war_gpu_floyd.py:95-105): plays, with Floyd's
  * tortoise and hare, every position of the job whose seeded hash falls in the sample, and fills the
  * s_* fields of out (the rest is zero).  They must equal the s_* fields of war_enumerate /
