@@ -224,6 +224,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain-kernel comparison run")
     args = ap.parse_args()
 
     rank, ws, local = dist_init()
@@ -313,6 +314,16 @@ def main():
         e2e = {"value": total / e2e_s, "unit": "positions/s" if mode else "deals/s", "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "api": "war_gpu.run" if ws == 1 else "warlib.enumerate_job"}
 
+    # the plain kernel (the reference's per-thread rank blocks, restated for sm_100a) on the same job,
+    # once, outside the timed region: the batched-versus-plain ratio
+    plain = None
+    if not args.no_plain and ws == 1:
+        warlib.set_stream(stream.cuda_stream)
+        rp = warlib.enumerate_plain(job)
+        assert (rp.cyc, rp.done, rp.maxfin) == (res.cyc, res.done, res.maxfin), "plain and refill kernels disagree"
+        plain = {"value": (hi - lo) / (rp.kernel_ms * 1e-3), "kernel_ms": rp.kernel_ms, "turns": rp.turns,
+                 "batched_over_plain": rp.kernel_ms / kernel_ms}
+
     if rank == 0:
         issue_peak, alu_peak = warlib.measure_int_peak()
         achieved = turns * K_OPS_PER_TURN / (kernel_ms * 1e-3)    # algorithmic int ops/s of the refill kernel
@@ -340,6 +351,8 @@ def main():
         }
         if e2e:
             line["e2e"] = e2e
+        if plain:
+            line["plain_kernel"] = plain
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(w)
         print(json.dumps(line), flush=True)
