@@ -240,9 +240,10 @@ def main():
     import war_gpu
     w = WORKLOADS[args.workload]
     n, mode = w["n"], w["mode"]
+    import shard
     lo0, hi0 = w.get("lo", 0), w.get("hi", space(n, mode))
     total = hi0 - lo0
-    lo, hi = lo0 + total * rank // ws, lo0 + total * (rank + 1) // ws
+    lo, hi = shard.shard_range(lo0, hi0, rank, ws)
     job = warlib.make_job(n, mode, 0, w["flags"], lo, hi, hbins=w["hbins"], dbins=w.get("dbins", 0),
                           sample_ppm=w.get("sample_ppm", 0), seed=w.get("seed", 0))
     torch.cuda.set_device(local)
@@ -285,13 +286,10 @@ def main():
         assert r.done == results[0].done and r.cyc == results[0].cyc and r.maxfin == results[0].maxfin
     res = results[-1]
     acc = [res.cyc, res.done, res.maxfin, res.turns, res.distinct_min, res.oncycle]
-    if ws > 1:
-        import torch.distributed as dist
-        t = torch.tensor(acc[:2] + acc[3:], dtype=torch.int64, device="cuda")
-        dist.all_reduce(t)
-        m = torch.tensor([acc[2]], dtype=torch.int64, device="cuda")
-        dist.all_reduce(m, op=dist.ReduceOp.MAX)
-        acc = [int(t[0]), int(t[1]), int(m[0]), int(t[2]), int(t[3]), int(t[4])]
+    if ws > 1:   # the one exchange of the sharded path: combine the per-rank results
+        import shard
+        d = shard.allreduce_result(shard.result_to_dict(res), device="cuda")
+        acc = [d["cyc"], d["done"], d["maxfin"], d["turns"], d["distinct_min"], d["oncycle"]]
     check = verify(w, acc, res if ws == 1 else None) if "lo" not in w else "slice (no recorded total)"
 
     # e2e through the public drop-in API (war_gpu.run), host buffers, copies inside the timed region

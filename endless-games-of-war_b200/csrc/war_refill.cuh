@@ -1,0 +1,351 @@
+// war_refill.cuh — the refill loop shared by the persistent kernel (war_batched.cu) and the serving
+// kernel (war_server.cu).
+//
+// The reference gives every thread 256 consecutive deals and plays them one after another, so a warp
+// runs each deal slot as long as its longest game (gpu/war_gpu.py:149-165).  Here every lane keeps
+// G games in flight and steps all of them every iteration; a lane whose game is decided records it and
+// loads its next position at once, so uneven game lengths do not idle the warp.  The grid is
+// persistent (SMs x resident blocks) and lanes pull work units from one global atomic counter.
+//
+// Enumeration inside a unit: a unit is the block of j! consecutive lexicographic ranks that share a
+// prefix, i.e. every order of the last j positions.  The counts are sums and maxima over that SET, so
+// the lane walks it in Heap's order (one transposition per step, the counter packed in nibbles)
+// instead of lexicographic order; the set is the same.  Deals are held in a split layout: deck
+// position p lives in slot (p>>1) + 8*(p&1), so player 1's cards are the low 32 bits and player 2's
+// the high 32 bits and dealing is two ORs (war_cycles, gpu/war_gpu.py:98-107).
+//
+// Cycle detection is Brent (gpu/war_gpu.py:77-96) with the tortoise saved at steps W, 3W, 7W, ...;
+// W = 1 is the reference's schedule.  With W >= lam the first window compares every state with the
+// starting position itself, so a canonical start that lies on its cycle is recognised at no cost,
+// and the distinct-cycle walk of gpu/war_gpu.py:224-234 runs only for those few positions.
+#pragma once
+#include "war_kernels.cuh"
+
+namespace war {
+
+
+struct Enum {
+    u64 P;       // current order: split layout (deals) or packed q (canon)
+    u32 ctr;     // Heap counter, digit i in nibble i
+    u32 full;    // counter value of the unit's last order
+    u32 base;    // first permuted position, M - j
+    u32 k, k0, k1;
+    bool live;   // P (and k) name the next unplayed position
+};
+
+template <bool CANON>
+__device__ __forceinline__ u32 pos_shift(u32 p) {
+    return CANON ? 4u * p : 4u * ((p >> 1) + ((p & 1u) << 3));
+}
+
+__device__ __forceinline__ u32 heap_full(u32 j) {
+    u32 f = 0;
+    for (u32 i = 1; i < j; i++) f |= i << (4u * i);
+    return f;
+}
+
+template <bool CANON>
+__device__ __forceinline__ bool fetch_unit(Enum& E, const BatchArgs& a, u64* counter) {
+    u64 u = atomicAdd(counter, 1ull);
+    if (u >= a.n_units) return false;
+    u64 r;
+    u32 j, k0, k1;
+    if (u < a.main_count) {
+        j = (u32)a.m; r = (a.main_base + u) * a.fact[a.m]; k0 = 0; k1 = (u32)a.n - 1u;
+    } else {
+        const Unit U = a.units[u - a.main_count];
+        r = U.r; j = U.j; k0 = U.k0; k1 = U.k1;
+    }
+    const int M = CANON ? a.n - 1 : a.n;
+    u64 p = unrank_packed(r, M, a.fact);
+    if (!CANON) p = compact_even_nibbles(p) | (compact_even_nibbles(p >> 4) << 32);
+    E.P = p;
+    E.ctr = 0;
+    E.full = heap_full(j);
+    E.base = (u32)M - j;
+    E.k0 = k0; E.k1 = k1; E.k = k0;
+    E.live = true;
+    return true;
+}
+
+// Heap's algorithm, one output: the lowest digit i with ctr[i] < i increments, the digits below it
+// reset to 0, and position i swaps with position 0 (i even) or ctr[i] (i odd).  False after the last.
+template <bool CANON>
+__device__ __forceinline__ bool heap_step(Enum& E) {
+    u32 x = E.ctr ^ E.full;
+    if (x == 0u) return false;
+    u32 i = (u32)(__ffs((int)x) - 1) >> 2;
+    u32 ci = (E.ctr >> (4u * i)) & 15u;
+    u32 o = (i & 1u) ? ci : 0u;
+    E.P = swap_nibbles(E.P, pos_shift<CANON>(E.base + i), pos_shift<CANON>(E.base + o));
+    E.ctr = ((E.ctr >> (4u * i)) + 1u) << (4u * i);
+    return true;
+}
+
+struct DealConst { u64 s1, s2; u32 q0, pat32; };
+
+// Next deal of the lane (deals mode); false when the lane has no work left.
+__device__ __forceinline__ bool next_deal(Enum& E, const BatchArgs& a, u64* counter, const DealConst& c, u64& w1,
+                                          u64& w2, u32& q) {
+    for (;;) {
+        if (!E.live && !fetch_unit<false>(E, a, counter)) return false;
+        u64 D = E.P;
+        E.live = heap_step<false>(E);
+        if (a.half) {   // gpu/war_gpu.py:151-154: card n-1 dealt to player 1
+            u32 x = (u32)D ^ c.pat32;
+            if (((x - 0x11111111u) & ~x & 0x88888888u) == 0u) continue;
+        }
+        w1 = (D & 0xFFFFFFFFull) | c.s1;
+        w2 = (D >> 32) | c.s2;
+        q = c.q0;
+        return true;
+    }
+}
+
+// Next canonical position of the lane.
+__device__ __forceinline__ bool next_canon(Enum& E, const BatchArgs& a, u64* counter, u64& w1, u64& w2, u32& q) {
+    if (!E.live && !fetch_unit<true>(E, a, counter)) return false;
+    canon_position(E.P, (u32)a.n, E.k, w1, w2, q);
+    if (++E.k == E.k1) {
+        E.k = E.k0;
+        E.live = heap_step<true>(E);
+    }
+    return true;
+}
+
+// One game slot.  EXTRA keeps the start position and the sample bit (distinct walk, sample);
+// SHAPE keeps the run tracker of the current tortoise window.
+enum { ST_ACTIVE = 0, ST_WAITING = 1, ST_RETIRED = 2 };
+
+template <bool EXTRA, bool SHAPE>
+struct Game {
+    u64 w1, w2, t1, t2;
+    u32 q, rounds, next, st;
+    // EXTRA
+    u64 s1, s2; u32 sq; bool sampled;
+    // SHAPE: run tracker since the last tortoise save
+    u32 cur, first_run; bool first, prev, started, ok;
+};
+
+// The refill loop of one block: lanes take work units from *counter (shared by every block that works on
+// the same unit list), play them and add the block's results to *acc.  sh: hbins + WAR_EBINS u32 words of
+// shared memory.  Used by the persistent kernel (one job, all blocks) and by the serving kernel (one task
+// of one job per block).
+template <int RULE, int G, bool CANON, bool SHAPE, bool EXTRA, int TV>
+__device__ __forceinline__ void refill_body(const BatchArgs& a, DevAcc* __restrict__ acc, u64* __restrict__ counter,
+                                            u32* sh) {
+    u32* shh = sh;
+    u32* she = sh + a.hbins;
+    for (int b = threadIdx.x; b < a.hbins + WAR_EBINS; b += blockDim.x) sh[b] = 0;
+    __syncthreads();
+
+    const u32 n = (u32)a.n, n4 = 4u * n, k4m4 = 4u * (n - 1u), W = (u32)a.W;
+    const TurnK K = a.tk;
+    // TV = 0: war_turn (q = 4*len1); TV = 1: war_turn_fma (q holds qq = 4*len1 - 2n)
+    const u32 qshift = TV ? 2u * n : 0u;
+    const u32 hb1 = a.hbins > 0 ? (u32)(a.hbins - 1) : 0u;
+    DealConst dc;
+    dc.s1 = sentinel_bit((n + 1u) / 2u);
+    dc.s2 = sentinel_bit(n / 2u);
+    dc.q0 = 4u * ((n + 1u) / 2u);
+    dc.pat32 = 0x11111111u * (n - 1u);
+
+    Enum E;
+    E.live = false;
+    Game<EXTRA, SHAPE> g[G];
+    // Per-lane totals.  A launch plays fewer than 2^32 games in all, so no lane's 32-bit turn total wraps.
+    u32 cyc = 0, done = 0, maxfin = 0, capped = 0, turns = 0;
+    u32 sc = 0, scy = 0, slam = 0, slen = 0, smax = 0, oncyc = 0, dmin = 0, nonstd = 0, unchk = 0;
+
+    // Game slot states: ACTIVE (being played), WAITING (decided and recorded, frozen until the warp
+    // refills), RETIRED (no work left).  A frozen slot holds two empty words and q far out of range, so
+    // the turn step leaves it unchanged (the pushed pair shifts out, shl64 gives 0).
+    // A frozen slot can never signal: its low words differ from its tortoise's, its next checkpoint is
+    // never reached, and its length offset is odd and far from both ends.  Every turn moves the offset by
+    // 4, so it stays odd: never 0 or 4n, and its square (multiply-add form) is odd, never (2n)^2.  With
+    // both words empty the pushed pair lands beyond bit 63 and the words stay 0.
+    auto freeze = [&](Game<EXTRA, SHAPE>& x) {
+        x.w1 = 0ull; x.w2 = 0ull; x.q = 0x80000001u; x.t1 = 1ull; x.t2 = 1ull; x.next = 0xFFFFFFFFu;
+    };
+    auto start_game = [&](Game<EXTRA, SHAPE>& x) {
+        bool ok = CANON ? next_canon(E, a, counter, x.w1, x.w2, x.q) : next_deal(E, a, counter, dc, x.w1, x.w2, x.q);
+        x.st = ok ? ST_ACTIVE : ST_RETIRED;
+        done += ok ? 1u : 0u;
+        x.t1 = x.w1; x.t2 = x.w2; x.rounds = 0; x.next = W;
+        if (EXTRA) {
+            x.s1 = x.w1; x.s2 = x.w2; x.sq = x.q;
+            x.sampled = a.sample && ok && war_pick(a.seed, a.thr, x.w1, x.w2);
+        }
+        if (SHAPE) x.cur = 0;
+        x.q -= qshift;
+        if (!ok) freeze(x);
+    };
+
+#pragma unroll
+    for (int i = 0; i < G; i++) start_game(g[i]);
+
+    // The warp leaves the loop once none of its lanes holds an active or waiting game.  That test runs
+    // whenever a slot changes state (a game decided or abandoned at the cap), and once here for warps that
+    // got no work at all.  Decided games wait, frozen, until `defer` lanes of the warp are waiting (or
+    // none is playing); then all of them load their next position together, so the refill code runs
+    // with many lanes at once instead of one.
+    const int defer = a.defer > 0 ? a.defer : 1;
+    bool alive0 = false;
+#pragma unroll
+    for (int i = 0; i < G; i++) alive0 |= g[i].st == ST_ACTIVE;
+    bool running = __any_sync(WAR_FULL_MASK, alive0);
+
+    while (running) {
+        bool fin[G];
+        bool anyfin = false;
+#pragma unroll
+        for (int i = 0; i < G; i++) {
+            Game<EXTRA, SHAPE>& x = g[i];
+            bool p1, en;
+            if (TV == 1) {
+                p1 = war_turn_fma<RULE>(x.w1, x.w2, x.q, K);
+                x.rounds = x.rounds * K.one + K.one;
+                en = x.q * x.q == K.end2;
+            } else {
+                p1 = war_turn<RULE>(x.w1, x.w2, x.q, k4m4);
+                x.rounds++;
+                en = (x.q == 0u) | (x.q == n4);
+            }
+            // Cycle candidate: the low words of both piles equal the tortoise's.  Exact equality of the
+            // high words is checked when the game is recorded; a candidate that fails it plays on.
+            bool cy = ((u32)x.w1 == (u32)x.t1) & ((u32)x.w2 == (u32)x.t2);
+            if (SHAPE) {
+                if (x.cur == 0u) { x.first = p1; x.prev = p1; x.cur = 1u; x.first_run = 0u; x.started = false; x.ok = true; }
+                else if (p1 == x.prev) x.cur++;
+                else {
+                    if (!x.started) { x.first_run = x.cur; x.started = true; }
+                    else x.ok = x.ok && (x.cur == (u32)a.blk);
+                    x.cur = 1u; x.prev = p1;
+                }
+            }
+            if (x.rounds == x.next && !(cy | en)) {   // a decided game keeps its tortoise (the record reads it)
+                if (x.next > WAR_TURN_CAP) {
+                    if (x.st == ST_ACTIVE) { capped++; x.st = ST_WAITING; freeze(x); anyfin = true; }
+                } else {
+                    x.t1 = x.w1; x.t2 = x.w2; x.next = 2u * x.next + W;
+                    if (SHAPE) x.cur = 0u;
+                }
+            }
+            fin[i] = cy | en;
+            anyfin |= fin[i];
+        }
+        if (__any_sync(WAR_FULL_MASK, anyfin)) {
+#pragma unroll
+            for (int i = 0; i < G; i++) {
+                Game<EXTRA, SHAPE>& x = g[i];
+                bool rec = fin[i];
+                if (rec) {
+                    const bool en = TV ? (x.q * x.q == K.end2) : ((x.q == 0u) | (x.q == n4));
+                    if (!en && !((x.w1 == x.t1) & (x.w2 == x.t2))) {
+                        // low words matched by chance: play on, with the tortoise save this step skipped
+                        rec = false;
+                        if (x.rounds == x.next) {
+                            x.t1 = x.w1; x.t2 = x.w2; x.next = 2u * x.next + W;
+                            if (SHAPE) x.cur = 0u;
+                        }
+                    }
+                }
+                if (rec) {
+                    const bool cy = (x.w1 == x.t1) & (x.w2 == x.t2);
+                    turns += x.rounds;
+                    const u32 lam = x.rounds - ((x.next - W) >> 1);
+                    if (cy) {
+                        cyc++;
+                        if (a.hbins) atomicAdd(&shh[lam < hb1 ? lam : hb1], 1u);
+                        if (CANON && EXTRA && a.distinct) {
+                            const u32 tstep = (x.next - W) >> 1;
+                            bool on = (tstep == 0u) ? true
+                                    : (lam <= W ? false : on_cycle_walk<RULE>(x.s1, x.s2, x.sq, n, lam));
+                            if (on) {
+                                CycleWalk cw = cycle_walk<RULE>(x.s1, x.s2, x.sq, n, lam);
+                                oncyc++;
+                                if (cw.is_min) dmin++;
+                                if (a.dbins) {
+                                    u32 d = cw.sym ? cw.c1 : cw.c1 + cw.c2;
+                                    u32 db1 = (u32)(a.dbins - 1);
+                                    atomicAdd(&acc->dhist[d < db1 ? d : db1], 1ull);
+                                }
+                            }
+                        }
+                        if (SHAPE) {
+                            if (lam > 512u) unchk++;
+                            else {
+                                bool ok = x.started && x.ok;
+                                if (x.started) {
+                                    if (x.prev == x.first) ok = ok && (x.cur + x.first_run == (u32)a.blk);
+                                    else ok = ok && (x.cur == (u32)a.blk) && (x.first_run == (u32)a.blk);
+                                }
+                                if (!ok) nonstd++;
+                            }
+                        }
+                    } else {
+                        if (x.rounds > maxfin) maxfin = x.rounds;
+                        atomicAdd(&she[x.rounds < WAR_EBINS - 1 ? x.rounds : WAR_EBINS - 1], 1u);
+                    }
+                    if (EXTRA && x.sampled) {
+                        sc++;
+                        if (cy) { scy++; slam += lam; }
+                        else { slen += x.rounds; if (x.rounds > smax) smax = x.rounds; }
+                    }
+                    x.st = ST_WAITING;
+                    freeze(x);
+                }
+            }
+            bool waiting = false, playing = false;
+#pragma unroll
+            for (int i = 0; i < G; i++) { waiting |= g[i].st == ST_WAITING; playing |= g[i].st == ST_ACTIVE; }
+            const u32 wb = __ballot_sync(WAR_FULL_MASK, waiting);
+            const u32 pb = __ballot_sync(WAR_FULL_MASK, playing);
+            if (__popc(wb) >= defer || pb == 0u) {
+                if (waiting) {
+#pragma unroll
+                    for (int i = 0; i < G; i++)
+                        if (g[i].st == ST_WAITING) start_game(g[i]);
+                }
+                playing = false;
+#pragma unroll
+                for (int i = 0; i < G; i++) playing |= g[i].st == ST_ACTIVE;
+                running = __any_sync(WAR_FULL_MASK, playing);
+            }
+        }
+    }
+
+    u64 v_cyc = warp_sum(cyc), v_done = warp_sum(done), v_turns = warp_sum((u64)turns), v_max = warp_max(maxfin);
+    u64 v_cap = warp_sum(capped);
+    if ((threadIdx.x & 31) == 0) {
+        if (v_cyc) atomicAdd(&acc->cyc, v_cyc);
+        if (v_done) atomicAdd(&acc->done, v_done);
+        if (v_turns) atomicAdd(&acc->turns, v_turns);
+        if (v_max) atomicMax(&acc->maxfin, v_max);
+        if (v_cap) atomicAdd(&acc->status, v_cap);
+    }
+    if (EXTRA) {
+        u64 v_sc = warp_sum(sc), v_scy = warp_sum(scy), v_slam = warp_sum(slam), v_slen = warp_sum(slen);
+        u64 v_smax = warp_max(smax), v_on = warp_sum(oncyc), v_dmin = warp_sum(dmin);
+        if ((threadIdx.x & 31) == 0) {
+            if (v_sc) {
+                atomicAdd(&acc->s_count, v_sc); atomicAdd(&acc->s_cyc, v_scy); atomicAdd(&acc->s_lamsum, v_slam);
+                atomicAdd(&acc->s_lensum, v_slen); atomicMax(&acc->s_maxfin, v_smax);
+            }
+            if (v_on) atomicAdd(&acc->oncycle, v_on);
+            if (v_dmin) atomicAdd(&acc->distinct_min, v_dmin);
+        }
+    }
+    if (SHAPE) {
+        u64 v_ns = warp_sum(nonstd), v_un = warp_sum(unchk);
+        if ((threadIdx.x & 31) == 0) {
+            if (v_ns) atomicAdd(&acc->shape_nonstd, v_ns);
+            if (v_un) atomicAdd(&acc->shape_unchecked, v_un);
+        }
+    }
+    __syncthreads();
+    flush_hist(shh, acc->hist, a.hbins);
+    flush_hist(she, acc->endhist, WAR_EBINS);
+}
+
+}  // namespace war
