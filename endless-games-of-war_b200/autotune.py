@@ -9,7 +9,7 @@ at a time, over
     blocks_per_sm  resident blocks (0 = as many as fit)
     window         Brent's first tortoise window                         (8..128)
     defer          lanes that wait, decided, before the warp refills     (1..8)
-    variant        turn step form: logic/shift (0) or multiply-add (1)
+    variant        bit 0: multiply-add turn form; bit 1: latched records serviced every `defer` iterations
 Every configuration must return exactly the same counts as the first one; a mismatch raises.  The best
 configuration is stored in tune_cache.json next to this file, keyed by GPU name, n, mode, rule and flags.
 
@@ -33,8 +33,8 @@ SPACE = {
     "threads": [128, 256, 512, 1024],
     "blocks_per_sm": [0, 1, 2, 3, 4],
     "window": [8, 16, 32, 64, 128],
-    "defer": [1, 2, 4, 6, 8, 12, 16, 24],
-    "variant": [0, 1],
+    "defer": [1, 2, 4, 6, 8, 12, 16, 24, 32],
+    "variant": [0, 1, 2, 3],
 }
 DEFAULT = {"block_m": 5, "games": 2, "threads": 512, "blocks_per_sm": 0, "window": 32, "defer": 8, "variant": 1}
 

@@ -4,32 +4,38 @@
 
 namespace war {
 
-template <int RULE, int G, bool CANON, bool SHAPE, bool EXTRA, int TV>
+template <int RULE, int G, bool CANON, bool SHAPE, bool EXTRA, int V>
 __global__ void __launch_bounds__(G == 1 ? 1024 : 512) batched_kernel(const __grid_constant__ BatchArgs a,
                                                                      DevAcc* __restrict__ acc) {
     extern __shared__ u32 sh[];
-    refill_body<RULE, G, CANON, SHAPE, EXTRA, TV>(a, acc, &acc->work_next, sh);
+    refill_dispatch<RULE, G, CANON, SHAPE, EXTRA, V>(a, acc, &acc->work_next, sh);
 }
 
 // ---- dispatch over the compiled variants ----------------------------------------------------------
 
 typedef void (*BatchedFn)(const BatchArgs, DevAcc*);
 
-template <int RULE, int G, int TV>
+template <int RULE, int G, int V>
 static BatchedFn pick_g(int canon, int shape, int extra) {
-    if (!canon) return extra ? batched_kernel<RULE, G, false, false, true, TV> : batched_kernel<RULE, G, false, false, false, TV>;
-    if (shape) return extra ? batched_kernel<RULE, G, true, true, true, TV> : batched_kernel<RULE, G, true, true, false, TV>;
-    return extra ? batched_kernel<RULE, G, true, false, true, TV> : batched_kernel<RULE, G, true, false, false, TV>;
+    if (!canon) return extra ? batched_kernel<RULE, G, false, false, true, V> : batched_kernel<RULE, G, false, false, false, V>;
+    if (shape) return extra ? batched_kernel<RULE, G, true, true, true, V> : batched_kernel<RULE, G, true, true, false, V>;
+    return extra ? batched_kernel<RULE, G, true, false, true, V> : batched_kernel<RULE, G, true, false, false, V>;
 }
 
-template <int TV>
-static BatchedFn pick_tv(int canon, int rule, int shape, int extra, int games) {
-    if (rule) return games == 2 ? pick_g<1, 2, TV>(canon, shape, extra) : pick_g<1, 1, TV>(canon, shape, extra);
-    return games == 2 ? pick_g<0, 2, TV>(canon, shape, extra) : pick_g<0, 1, TV>(canon, shape, extra);
+template <int V>
+static BatchedFn pick_v(int canon, int rule, int shape, int extra, int games) {
+    if (rule) return games == 2 ? pick_g<1, 2, V>(canon, shape, extra) : pick_g<1, 1, V>(canon, shape, extra);
+    return games == 2 ? pick_g<0, 2, V>(canon, shape, extra) : pick_g<0, 1, V>(canon, shape, extra);
 }
 
+// variant: bit 0 = multiply-add turn form, bit 1 = latched records
 static BatchedFn pick(int canon, int rule, int shape, int extra, int games, int variant) {
-    return variant == 1 ? pick_tv<1>(canon, rule, shape, extra, games) : pick_tv<0>(canon, rule, shape, extra, games);
+    switch (variant) {
+        case 1: return pick_v<1>(canon, rule, shape, extra, games);
+        case 2: return pick_v<2>(canon, rule, shape, extra, games);
+        case 3: return pick_v<3>(canon, rule, shape, extra, games);
+        default: return pick_v<0>(canon, rule, shape, extra, games);
+    }
 }
 
 cudaError_t launch_batched(const BatchArgs& a, int canon, int rule, int shape, const BatchShape& bs, DevAcc* acc,

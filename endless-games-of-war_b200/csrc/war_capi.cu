@@ -205,7 +205,7 @@ int resolve_tune(const war_job* job, const war_tune* in, Tune& t) {
     if (t.block_m < 1 || t.block_m > 8) return fail(WAR_EINVAL, "tune.block_m=%d (1..8)", t.block_m);
     if (t.window < 1 || t.window > (1 << 16) || (t.window & (t.window - 1))) return fail(WAR_EINVAL, "tune.window=%d", t.window);
     if (t.defer < 1 || t.defer > 32) return fail(WAR_EINVAL, "tune.defer=%d (1..32)", t.defer);
-    if (t.variant != 0 && t.variant != 1) return fail(WAR_EINVAL, "tune.variant=%d (0 or 1)", t.variant);
+    if (t.variant < 0 || t.variant > 3) return fail(WAR_EINVAL, "tune.variant=%d (0..3)", t.variant);
     const int M = canon ? job->n - 1 : job->n;
     if (t.block_m > M) t.block_m = M > 0 ? M : 1;
     int st = ensure_ready();

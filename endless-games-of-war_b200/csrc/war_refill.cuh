@@ -348,4 +348,178 @@ __device__ __forceinline__ void refill_body(const BatchArgs& a, DevAcc* __restri
     flush_hist(she, acc->endhist, WAR_EBINS);
 }
 
+// The same refill loop with the outcome of each game latched instead of recorded at once.  Every
+// iteration steps all G games of every lane without a branch or a warp vote; a game whose cycle or end
+// is found sets its `done` flag, which freezes its turn count and its tortoise (the game itself keeps
+// being stepped, harmlessly).  Every K = a.defer iterations (a multiple of 4) the warp services its
+// slots: each done game is recorded and replaced by the lane's next position.  The record and refill
+// code therefore runs once per K iterations with every lane that has a done game, instead of once per
+// decided game with one lane.  The cycle test compares all four words (no candidate to verify later).
+template <bool EXTRA>
+struct LGame {
+    u64 w1, w2, t1, t2;
+    u32 q, rounds, next, st;
+    bool done, kcy;     // decided; decided by a cycle (else by an end)
+    u64 s1, s2; u32 sq; bool sampled;
+};
+
+template <int RULE, int G, bool CANON, bool EXTRA, int TV>
+__device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __restrict__ acc, u64* __restrict__ counter,
+                                               u32* sh) {
+    u32* shh = sh;
+    u32* she = sh + a.hbins;
+    for (int b = threadIdx.x; b < a.hbins + WAR_EBINS; b += blockDim.x) sh[b] = 0;
+    __syncthreads();
+
+    const u32 n = (u32)a.n, n4 = 4u * n, k4m4 = 4u * (n - 1u), W = (u32)a.W;
+    const TurnK K = a.tk;
+    const u32 qshift = TV ? 2u * n : 0u;
+    const u32 hb1 = a.hbins > 0 ? (u32)(a.hbins - 1) : 0u;
+    const int period = a.defer > 4 ? (a.defer + 3) & ~3 : 4;
+    DealConst dc;
+    dc.s1 = sentinel_bit((n + 1u) / 2u);
+    dc.s2 = sentinel_bit(n / 2u);
+    dc.q0 = 4u * ((n + 1u) / 2u);
+    dc.pat32 = 0x11111111u * (n - 1u);
+
+    Enum E;
+    E.live = false;
+    LGame<EXTRA> g[G];
+    u32 cyc = 0, done = 0, maxfin = 0, capped = 0, turns = 0;
+    u32 sc = 0, scy = 0, slam = 0, slen = 0, smax = 0, oncyc = 0, dmin = 0;
+
+    auto start_game = [&](LGame<EXTRA>& x) {
+        bool ok = CANON ? next_canon(E, a, counter, x.w1, x.w2, x.q) : next_deal(E, a, counter, dc, x.w1, x.w2, x.q);
+        x.st = ok ? ST_ACTIVE : ST_RETIRED;
+        done += ok ? 1u : 0u;
+        x.t1 = x.w1; x.t2 = x.w2; x.rounds = 0; x.next = W;
+        x.done = !ok; x.kcy = false;
+        if (EXTRA) {
+            x.s1 = x.w1; x.s2 = x.w2; x.sq = x.q;
+            x.sampled = a.sample && ok && war_pick(a.seed, a.thr, x.w1, x.w2);
+        }
+        x.q -= qshift;
+    };
+
+#pragma unroll
+    for (int i = 0; i < G; i++) start_game(g[i]);
+    bool alive0 = false;
+#pragma unroll
+    for (int i = 0; i < G; i++) alive0 |= g[i].st == ST_ACTIVE;
+    bool running = __any_sync(WAR_FULL_MASK, alive0);
+
+    while (running) {
+        for (int k = 0; k < period; k += 4) {
+#pragma unroll
+            for (int u = 0; u < 4; u++) {
+#pragma unroll
+                for (int i = 0; i < G; i++) {
+                    LGame<EXTRA>& x = g[i];
+                    bool en;
+                    if (TV == 1) {
+                        war_turn_fma<RULE>(x.w1, x.w2, x.q, K);
+                        en = x.q * x.q == K.end2;
+                    } else {
+                        war_turn<RULE>(x.w1, x.w2, x.q, k4m4);
+                        en = (x.q == 0u) | (x.q == n4);
+                    }
+                    if (!x.done) x.rounds += K.one;
+                    const bool cy = (x.w1 == x.t1) & (x.w2 == x.t2);
+                    const bool fin = (cy | en) & !x.done;
+                    x.kcy = fin ? cy : x.kcy;
+                    x.done = x.done | fin;
+                    if (x.rounds == x.next && !x.done) {
+                        if (x.next > WAR_TURN_CAP) {   // abandon (never expected): counted, slot serviced as done
+                            capped++; x.done = true; x.st = ST_WAITING;
+                        } else {
+                            x.t1 = x.w1; x.t2 = x.w2; x.next = 2u * x.next + W;
+                        }
+                    }
+                }
+            }
+        }
+        // service: record every decided game, refill its slot
+        bool any = false;
+#pragma unroll
+        for (int i = 0; i < G; i++) any |= g[i].done & (g[i].st != ST_RETIRED);
+        if (__any_sync(WAR_FULL_MASK, any)) {
+#pragma unroll
+            for (int i = 0; i < G; i++) {
+                LGame<EXTRA>& x = g[i];
+                if (x.done & (x.st == ST_ACTIVE)) {
+                    const bool cy = x.kcy;
+                    turns += x.rounds;
+                    const u32 lam = x.rounds - ((x.next - W) >> 1);
+                    if (cy) {
+                        cyc++;
+                        if (a.hbins) atomicAdd(&shh[lam < hb1 ? lam : hb1], 1u);
+                        if (CANON && EXTRA && a.distinct) {
+                            const u32 tstep = (x.next - W) >> 1;
+                            bool on = (tstep == 0u) ? true
+                                    : (lam <= W ? false : on_cycle_walk<RULE>(x.s1, x.s2, x.sq, n, lam));
+                            if (on) {
+                                CycleWalk cw = cycle_walk<RULE>(x.s1, x.s2, x.sq, n, lam);
+                                oncyc++;
+                                if (cw.is_min) dmin++;
+                                if (a.dbins) {
+                                    u32 d = cw.sym ? cw.c1 : cw.c1 + cw.c2;
+                                    u32 db1 = (u32)(a.dbins - 1);
+                                    atomicAdd(&acc->dhist[d < db1 ? d : db1], 1ull);
+                                }
+                            }
+                        }
+                    } else {
+                        if (x.rounds > maxfin) maxfin = x.rounds;
+                        atomicAdd(&she[x.rounds < WAR_EBINS - 1 ? x.rounds : WAR_EBINS - 1], 1u);
+                    }
+                    if (EXTRA && x.sampled) {
+                        sc++;
+                        if (cy) { scy++; slam += lam; }
+                        else { slen += x.rounds; if (x.rounds > smax) smax = x.rounds; }
+                    }
+                }
+                if (x.done & (x.st != ST_RETIRED)) start_game(x);
+            }
+            bool playing = false;
+#pragma unroll
+            for (int i = 0; i < G; i++) playing |= g[i].st == ST_ACTIVE;
+            running = __any_sync(WAR_FULL_MASK, playing);
+        }
+    }
+
+    u64 v_cyc = warp_sum(cyc), v_done = warp_sum(done), v_turns = warp_sum((u64)turns), v_max = warp_max(maxfin);
+    u64 v_cap = warp_sum(capped);
+    if ((threadIdx.x & 31) == 0) {
+        if (v_cyc) atomicAdd(&acc->cyc, v_cyc);
+        if (v_done) atomicAdd(&acc->done, v_done);
+        if (v_turns) atomicAdd(&acc->turns, v_turns);
+        if (v_max) atomicMax(&acc->maxfin, v_max);
+        if (v_cap) atomicAdd(&acc->status, v_cap);
+    }
+    if (EXTRA) {
+        u64 v_sc = warp_sum(sc), v_scy = warp_sum(scy), v_slam = warp_sum(slam), v_slen = warp_sum(slen);
+        u64 v_smax = warp_max(smax), v_on = warp_sum(oncyc), v_dmin = warp_sum(dmin);
+        if ((threadIdx.x & 31) == 0) {
+            if (v_sc) {
+                atomicAdd(&acc->s_count, v_sc); atomicAdd(&acc->s_cyc, v_scy); atomicAdd(&acc->s_lamsum, v_slam);
+                atomicAdd(&acc->s_lensum, v_slen); atomicMax(&acc->s_maxfin, v_smax);
+            }
+            if (v_on) atomicAdd(&acc->oncycle, v_on);
+            if (v_dmin) atomicAdd(&acc->distinct_min, v_dmin);
+        }
+    }
+    __syncthreads();
+    flush_hist(shh, acc->hist, a.hbins);
+    flush_hist(she, acc->endhist, WAR_EBINS);
+}
+
+// Dispatch: variant V selects the turn form (V & 1: multiply-add) and the record scheme (V & 2: latched);
+// the loop-shape tracker needs the immediate scheme.
+template <int RULE, int G, bool CANON, bool SHAPE, bool EXTRA, int V>
+__device__ __forceinline__ void refill_dispatch(const BatchArgs& a, DevAcc* __restrict__ acc, u64* __restrict__ counter,
+                                                u32* sh) {
+    if constexpr (SHAPE || (V & 2) == 0) refill_body<RULE, G, CANON, SHAPE, EXTRA, V & 1>(a, acc, counter, sh);
+    else refill_latched<RULE, G, CANON, EXTRA, V & 1>(a, acc, counter, sh);
+}
+
 }  // namespace war

@@ -33,7 +33,7 @@ struct ServeTask {
     u64 counter;      // the task's work-unit counter (zero when uploaded)
 };
 
-template <int RULE, int G, bool CANON, bool SHAPE, bool EXTRA, int TV>
+template <int RULE, int G, bool CANON, bool SHAPE, bool EXTRA, int V>
 __global__ void __launch_bounds__(G == 1 ? 1024 : 512) serve_kernel(ServeTask* __restrict__ tasks,
                                                                    DevAcc* __restrict__ slots) {
     extern __shared__ u32 sh[];
@@ -42,16 +42,16 @@ __global__ void __launch_bounds__(G == 1 ? 1024 : 512) serve_kernel(ServeTask* _
     const u32* src = (const u32*)&t->args;
     for (int i = threadIdx.x; i < (int)(sizeof(BatchArgs) / 4); i += blockDim.x) ((u32*)&A)[i] = src[i];
     __syncthreads();
-    refill_body<RULE, G, CANON, SHAPE, EXTRA, TV>(A, slots + t->slot, &t->counter, sh);
+    refill_dispatch<RULE, G, CANON, SHAPE, EXTRA, V>(A, slots + t->slot, &t->counter, sh);
 }
 
 typedef void (*ServeFn)(ServeTask*, DevAcc*);
 
-template <int RULE, int G, int TV>
+template <int RULE, int G, int V>
 static ServeFn serve_pick(bool canon, bool shape, bool extra) {
-    if (!canon) return extra ? serve_kernel<RULE, G, false, false, true, TV> : serve_kernel<RULE, G, false, false, false, TV>;
-    if (shape) return extra ? serve_kernel<RULE, G, true, true, true, TV> : serve_kernel<RULE, G, true, true, false, TV>;
-    return extra ? serve_kernel<RULE, G, true, false, true, TV> : serve_kernel<RULE, G, true, false, false, TV>;
+    if (!canon) return extra ? serve_kernel<RULE, G, false, false, true, V> : serve_kernel<RULE, G, false, false, false, V>;
+    if (shape) return extra ? serve_kernel<RULE, G, true, true, true, V> : serve_kernel<RULE, G, true, true, false, V>;
+    return extra ? serve_kernel<RULE, G, true, false, true, V> : serve_kernel<RULE, G, true, false, false, V>;
 }
 
 // Launch shapes of the serving kernel: deals 2 games per thread, 128-thread blocks; canonical positions

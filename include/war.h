@@ -77,8 +77,10 @@ typedef struct war_tune {
     int32_t games;         /* games in flight per thread: 1 or 2 */
     int32_t block_m;       /* each work unit covers m! consecutive ranks (deals) or m! orders x splits (canon); 1..8 */
     int32_t window;        /* Brent first tortoise window (power of two); 1 = the reference's schedule */
-    int32_t defer;         /* lanes of a warp that wait, decided, before the warp refills them (1..32) */
-    int32_t variant;       /* turn step: 0 = logic/shift form, 1 = multiply-add form (same results) */
+    int32_t defer;         /* immediate records: lanes that wait, decided, before the warp refills them (1..32);
+                              latched records: iterations between services (rounded up to a multiple of 4) */
+    int32_t variant;       /* bit 0: multiply-add turn form (else logic/shift); bit 1: outcomes latched and
+                              recorded every `defer` iterations (else recorded at once); same results */
     int32_t reserved;
 } war_tune;
 

@@ -81,7 +81,8 @@ def test_random_ranges(wl, oracle, mode):
                                   dict(block_m=3), dict(block_m=8), dict(window=64), dict(window=256),
                                   dict(blocks_per_sm=1), dict(games=2, threads=512, block_m=7, window=32),
                                   dict(defer=4), dict(defer=32), dict(variant=1), dict(variant=1, games=2, defer=3),
-                                  dict(variant=1, window=1, threads=128)])
+                                  dict(variant=1, window=1, threads=128), dict(variant=2), dict(variant=3, games=2, defer=16),
+                                  dict(variant=3, defer=4, threads=1024), dict(variant=2, window=1, defer=32, games=2)])
 def test_tunes_agree(wl, oracle, tune):
     for job in (wl.make_job(11, rule=0, hbins=64), wl.make_job(10, wl.CANON, rule=1, flags=wl.F_DISTINCT | wl.F_SHAPE,
                                                                  hbins=256, dbins=64)):
