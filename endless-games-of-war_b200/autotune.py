@@ -9,7 +9,8 @@ at a time, over
     blocks_per_sm  resident blocks (0 = as many as fit)
     window         Brent's first tortoise window                         (8..128)
     defer          lanes that wait, decided, before the warp refills     (1..8)
-    variant        bit 0: multiply-add turn form; bit 1: latched records serviced every `defer` iterations
+    variant        bit 0: multiply-add turn form; bit 1: latched records serviced every `defer` iterations;
+                   bit 2: cycle memo (deals)
 Every configuration must return exactly the same counts as the first one; a mismatch raises.  The best
 configuration is stored in tune_cache.json next to this file, keyed by GPU name, n, mode, rule and flags.
 
@@ -34,9 +35,11 @@ SPACE = {
     "blocks_per_sm": [0, 1, 2, 3, 4],
     "window": [8, 16, 32, 64, 128],
     "defer": [1, 2, 4, 6, 8, 12, 16, 24, 32],
-    "variant": [0, 1, 2, 3],
+    "variant": [0, 1, 2, 3, 6, 7],
+    "memo_bits": [22, 24, 26],
 }
-DEFAULT = {"block_m": 5, "games": 2, "threads": 512, "blocks_per_sm": 0, "window": 32, "defer": 8, "variant": 1}
+DEFAULT = {"block_m": 5, "games": 2, "threads": 512, "blocks_per_sm": 0, "window": 32, "defer": 8, "variant": 1,
+           "memo_bits": 24}
 
 
 def key(n, mode, rule, flags, device=None):
@@ -59,7 +62,7 @@ def cached_tune(n, mode, rule, flags):
         return None
     t = c["tune"]
     return warlib.make_tune(t["threads"], t["blocks_per_sm"], t["games"], t["block_m"], t["window"], t["defer"],
-                            t.get("variant", 0))
+                            t.get("variant", 0), t.get("memo_bits", 0))
 
 
 def _legal(n, mode, flags, cfg):
@@ -106,6 +109,9 @@ def autotune(n, mode=warlib.DEALS, rule=0, flags=0, slice_s=0.4, passes=2, verbo
     cur = dict(DEFAULT)
     if mode == warlib.CANON:
         cur.update(block_m=5, window=128 if flags & warlib.F_DISTINCT else 64)
+    stored = load_cache().get(key(n, mode, rule, flags))
+    if stored:   # start from the stored best
+        cur.update(stored["tune"])
     lo, hi = _slice(n, mode, rule, flags, slice_s, cur)
     job = warlib.make_job(n, mode, rule, flags, lo, hi, hbins=256, dbins=4096 if flags & warlib.F_DISTINCT else 0)
     best_ms, ref = measure(job, cur)

@@ -18,6 +18,7 @@ typedef void (*BatchedFn)(const BatchArgs, DevAcc*);
 template <int RULE, int G, int V>
 static BatchedFn pick_g(int canon, int shape, int extra) {
     if (!canon) return extra ? batched_kernel<RULE, G, false, false, true, V> : batched_kernel<RULE, G, false, false, false, V>;
+    if constexpr ((V & 4) != 0) return nullptr;   // the cycle memo serves deals only
     if (shape) return extra ? batched_kernel<RULE, G, true, true, true, V> : batched_kernel<RULE, G, true, true, false, V>;
     return extra ? batched_kernel<RULE, G, true, false, true, V> : batched_kernel<RULE, G, true, false, false, V>;
 }
@@ -28,12 +29,15 @@ static BatchedFn pick_v(int canon, int rule, int shape, int extra, int games) {
     return games == 2 ? pick_g<0, 2, V>(canon, shape, extra) : pick_g<0, 1, V>(canon, shape, extra);
 }
 
-// variant: bit 0 = multiply-add turn form, bit 1 = latched records
+// variant: bit 0 = multiply-add turn form, bit 1 = latched records, bit 2 = cycle memo (deals, latched)
 static BatchedFn pick(int canon, int rule, int shape, int extra, int games, int variant) {
+    if (canon || (variant & 2) == 0) variant &= 3;
     switch (variant) {
         case 1: return pick_v<1>(canon, rule, shape, extra, games);
         case 2: return pick_v<2>(canon, rule, shape, extra, games);
         case 3: return pick_v<3>(canon, rule, shape, extra, games);
+        case 6: return pick_v<6>(canon, rule, shape, extra, games);
+        case 7: return pick_v<7>(canon, rule, shape, extra, games);
         default: return pick_v<0>(canon, rule, shape, extra, games);
     }
 }

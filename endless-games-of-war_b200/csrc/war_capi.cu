@@ -200,12 +200,16 @@ int resolve_tune(const war_job* job, const war_tune* in, Tune& t) {
     t.window = (in && in->window) ? in->window : (canon ? 128 : 32);
     t.defer = (in && in->defer) ? in->defer : 1;
     t.variant = in ? in->variant : 0;
+    t.memo_bits = (in && in->memo_bits) ? in->memo_bits : 24;
     if (t.threads < 64 || t.threads > 1024 || (t.threads & 31)) return fail(WAR_EINVAL, "tune.threads=%d", t.threads);
     if (t.games != 1 && t.games != 2) return fail(WAR_EINVAL, "tune.games=%d (1 or 2)", t.games);
     if (t.block_m < 1 || t.block_m > 8) return fail(WAR_EINVAL, "tune.block_m=%d (1..8)", t.block_m);
     if (t.window < 1 || t.window > (1 << 16) || (t.window & (t.window - 1))) return fail(WAR_EINVAL, "tune.window=%d", t.window);
     if (t.defer < 1 || t.defer > 32) return fail(WAR_EINVAL, "tune.defer=%d (1..32)", t.defer);
-    if (t.variant < 0 || t.variant > 3) return fail(WAR_EINVAL, "tune.variant=%d (0..3)", t.variant);
+    if (t.variant < 0 || t.variant > 7) return fail(WAR_EINVAL, "tune.variant=%d (0..7)", t.variant);
+    if (t.memo_bits < 12 || t.memo_bits > 28) return fail(WAR_EINVAL, "tune.memo_bits=%d (12..28)", t.memo_bits);
+    // the cycle memo serves deals of 4..15 cards with latched records
+    if ((t.variant & 4) && (canon || !(t.variant & 2) || job->n < 4 || job->n > 15)) t.variant &= 3;
     const int M = canon ? job->n - 1 : job->n;
     if (t.block_m > M) t.block_m = M > 0 ? M : 1;
     int st = ensure_ready();
@@ -495,6 +499,23 @@ int war_enumerate(const war_job* job, const war_tune* tune, war_result* out) {
     a.seed = job->seed;
     a.thr = ((u64)job->sample_ppm << 32) / 1000000u;
     a.units = c.d_units;
+    if (t.variant & 4) {   // the cycle memo, cleared for this job
+        const size_t bytes = sizeof(u64) << t.memo_bits;
+        if (c.memo_bits != t.memo_bits) {
+            if (c.d_memo) cudaFree(c.d_memo);
+            c.d_memo = nullptr;
+            c.memo_bits = 0;
+            if ((e = cudaMalloc(&c.d_memo, bytes)) != cudaSuccess) {
+                c.d_memo = nullptr;
+                return cuda_fail(e, "cudaMalloc cycle memo");
+            }
+            c.memo_bits = t.memo_bits;
+        }
+        if ((e = cudaMemsetAsync(c.d_memo, 0, bytes, cur_stream())) != cudaSuccess)
+            return cuda_fail(e, "clear cycle memo");
+        a.memo = c.d_memo;
+        a.memo_bits = (u32)t.memo_bits;
+    }
     // Each launch plays fewer than 2^32 games, so the 32-bit per-block and per-lane counters cannot wrap.
     const u64 per_unit = fact(t.block_m) * p.games_per_order;
     const u64 max_units = std::max<u64>(1, ((1ull << 32) - (1ull << 24)) / per_unit);

@@ -18,6 +18,8 @@ struct Ctx {
     Unit* d_units = nullptr;        // extra work units of the running job
     ulonglong2* d_sample = nullptr; // Floyd sample buffer
     size_t sample_cap = 0;
+    u64* d_memo = nullptr;          // cycle memo table of the refill kernel (deals)
+    int memo_bits = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 
@@ -29,7 +31,7 @@ struct Plan {
 };
 
 struct Tune {
-    int threads, blocks_per_sm, games, block_m, window, defer, variant;
+    int threads, blocks_per_sm, games, block_m, window, defer, variant, memo_bits;
 };
 
 Ctx& ctx();

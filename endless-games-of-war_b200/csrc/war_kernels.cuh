@@ -36,6 +36,8 @@ struct BatchArgs {
     u64 seed, thr;
     TurnK tk;          // constants of war_turn_fma
     int n, m, hbins, dbins, blk, W, half, sample, distinct, defer;
+    u64* memo;         // cycle memo table (2^memo_bits words, 0 = empty), or null
+    u32 memo_bits, memo_pad;
 };
 
 struct CycleWalk { u32 c1, c2; bool sym, on, is_min; };

@@ -348,6 +348,60 @@ __device__ __forceinline__ void refill_body(const BatchArgs& a, DevAcc* __restri
     flush_hist(she, acc->endhist, WAR_EBINS);
 }
 
+// ---- cycle memo ---------------------------------------------------------------------------------------
+// Every cycle of a game contains "landmark" states, where card n-1 is on top of its holder's pile (card
+// n-1 never loses, and each pile is a queue, so every card reaches the top within one cycle).  The memo
+// holds the landmarks of the cycles found so far in the job.  A game that passes a landmark in the memo
+// is on that cycle: it never ends and its cycle length is the memo's, so it is decided then instead of
+// when Brent's test fires.  Brent keeps running for every game, so a cycle missing from the memo (not
+// found yet, or a full table) is still found exactly: the memo only decides games earlier.  War is the
+// same game with the players swapped (the winner's card, then the loser's, goes under the winner's
+// pile), so a landmark is stored once, with the holder of card n-1 as the first player.
+//
+// Entry (one 64-bit word): the holder's pile without its top card (which is n-1) followed by the other
+// pile, as 4(n-2) bits of nibbles (the last card is the one missing), then the holder's pile length in
+// 4 bits, then the cycle length in the remaining 64 - 4(n-1) bits.  The length field is at least 1, so
+// no entry is 0, which marks an empty slot.  n <= 15, cycle lengths below 2^(64 - 4(n-1)).
+//
+// The table is direct-mapped and written with a fire-and-forget atomic maximum: a slot wanted by two
+// landmarks keeps one whole entry of the two (the other is lost, which only means a later detection).
+// Inserts therefore never wait for memory and lookups are one load, with no probe chain.
+__device__ __forceinline__ u32 pile_len(u64 w) { return (63u - (u32)__clzll(w | 1ull)) >> 2; }
+
+// The key of the landmark where pile h (top card n-1) is the holder's and pile o the other's.
+__device__ __forceinline__ u64 memo_key(u64 h, u64 o, u32 n) {
+    const u32 lh = pile_len(h);
+    const u64 cat = (h ^ (1ull << (4u * lh))) | (o << (4u * lh));   // holder's cards, then the other's
+    const u32 kb = 4u * (n - 2u);
+    return ((cat >> 4) & ((1ull << kb) - 1ull)) | ((u64)lh << kb);
+}
+
+__device__ __forceinline__ u32 memo_slot(u64 key, u32 bits) {
+    return (u32)((key * 0x9E3779B97F4A7C15ull) >> (64u - bits));
+}
+
+// The atomic is skipped when the slot already holds this entry or a larger one (it would change
+// nothing), which keeps the games that find the same new cycle at once from queueing on its slots.
+__device__ __forceinline__ void memo_put(u64* T, u32 bits, u64 key, u32 lsh, u32 lam) {
+    unsigned long long* p = (unsigned long long*)T + memo_slot(key, bits);
+    const unsigned long long val = key | ((u64)lam << lsh);
+    if (__ldcg(p) < val) atomicMax(p, val);
+}
+
+// Walks the cycle of length lam through the state (w1, w2, q4 = 4*len1) once and stores its landmarks.
+template <int RULE>
+__device__ __noinline__ void memo_store_cycle(u64* T, u32 bits, u64 w1, u64 w2, u32 q4, u32 n, u32 lam) {
+    const u32 lsh = 4u * (n - 1u);
+    if (lam == 0u || (u64)lam >> (64u - lsh) != 0ull) return;
+    const u32 k4m4 = 4u * (n - 1u);
+    const u64 top = (u64)(n - 1u);
+    for (u32 t = 0; t < lam; t++) {
+        if ((w1 & 15ull) == top) memo_put(T, bits, memo_key(w1, w2, n), lsh, lam);
+        else if ((w2 & 15ull) == top) memo_put(T, bits, memo_key(w2, w1, n), lsh, lam);
+        war_turn<RULE>(w1, w2, q4, k4m4);
+    }
+}
+
 // The same refill loop with the outcome of each game latched instead of recorded at once.  Every
 // iteration steps all G games of every lane without a branch or a warp vote; a game whose cycle or end
 // is found sets its `done` flag, which freezes its turn count and its tortoise (the game itself keeps
@@ -355,15 +409,20 @@ __device__ __forceinline__ void refill_body(const BatchArgs& a, DevAcc* __restri
 // slots: each done game is recorded and replaced by the lane's next position.  The record and refill
 // code therefore runs once per K iterations with every lane that has a done game, instead of once per
 // decided game with one lane.  The cycle test compares all four words (no candidate to verify later).
-template <bool EXTRA>
+template <bool EXTRA, bool MEMO>
 struct LGame {
     u64 w1, w2, t1, t2;
     u32 q, rounds, next, st;
     bool done, kcy;     // decided; decided by a cycle (else by an end)
     u64 s1, s2; u32 sq; bool sampled;
+    u64 m1, m2;         // MEMO: the last landmark passed since the last lookup (m1 = 0: none)
+    u32 mlam;           // MEMO: cycle length given by the memo (0: decided by Brent)
 };
 
-template <int RULE, int G, bool CANON, bool EXTRA, int TV>
+// With MEMO, each turn also keeps the state before it when card n-1 is on top (a landmark), and every
+// service looks the kept landmark of each undecided game up in the memo; a game decided by Brent stores
+// its cycle's landmarks.
+template <int RULE, int G, bool CANON, bool EXTRA, int TV, bool MEMO>
 __device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __restrict__ acc, u64* __restrict__ counter,
                                                u32* sh) {
     u32* shh = sh;
@@ -384,16 +443,21 @@ __device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __res
 
     Enum E;
     E.live = false;
-    LGame<EXTRA> g[G];
+    LGame<EXTRA, MEMO> g[G];
     u32 cyc = 0, done = 0, maxfin = 0, capped = 0, turns = 0;
     u32 sc = 0, scy = 0, slam = 0, slen = 0, smax = 0, oncyc = 0, dmin = 0;
+    const u32 nm1 = n - 1u;
+    u64* const memo = MEMO ? a.memo : nullptr;
+    const u32 mbits = a.memo_bits, lsh = 4u * (n - 1u);
+    const u64 kmask = lsh < 64u ? (1ull << lsh) - 1ull : ~0ull;
 
-    auto start_game = [&](LGame<EXTRA>& x) {
+    auto start_game = [&](LGame<EXTRA, MEMO>& x) {
         bool ok = CANON ? next_canon(E, a, counter, x.w1, x.w2, x.q) : next_deal(E, a, counter, dc, x.w1, x.w2, x.q);
         x.st = ok ? ST_ACTIVE : ST_RETIRED;
         done += ok ? 1u : 0u;
         x.t1 = x.w1; x.t2 = x.w2; x.rounds = 0; x.next = W;
         x.done = !ok; x.kcy = false;
+        if (MEMO) { x.m1 = 0ull; x.m2 = 0ull; x.mlam = 0u; }
         if (EXTRA) {
             x.s1 = x.w1; x.s2 = x.w2; x.sq = x.q;
             x.sampled = a.sample && ok && war_pick(a.seed, a.thr, x.w1, x.w2);
@@ -414,7 +478,13 @@ __device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __res
             for (int u = 0; u < 4; u++) {
 #pragma unroll
                 for (int i = 0; i < G; i++) {
-                    LGame<EXTRA>& x = g[i];
+                    LGame<EXTRA, MEMO>& x = g[i];
+                    if (MEMO) {
+                        const u32 c1 = (u32)x.w1 & 15u, c2 = (u32)x.w2 & 15u;
+                        const bool lm = max(c1, c2) == nm1;
+                        x.m1 = lm ? x.w1 : x.m1;
+                        x.m2 = lm ? x.w2 : x.m2;
+                    }
                     bool en;
                     if (TV == 1) {
                         war_turn_fma<RULE>(x.w1, x.w2, x.q, K);
@@ -438,6 +508,25 @@ __device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __res
                 }
             }
         }
+        if (MEMO && memo != nullptr) {   // look up the kept landmarks: the loads of all G games first
+            u64 key[G], e[G];
+            bool look[G];
+#pragma unroll
+            for (int i = 0; i < G; i++) {
+                LGame<EXTRA, MEMO>& x = g[i];
+                look[i] = !x.done & (x.m1 != 0ull);
+                const bool h1 = ((u32)x.m1 & 15u) == nm1;
+                key[i] = memo_key(h1 ? x.m1 : x.m2, h1 ? x.m2 : x.m1, n);
+                e[i] = look[i] ? __ldcg((const unsigned long long*)memo + memo_slot(key[i], mbits)) : 0ull;
+                x.m1 = 0ull;
+            }
+#pragma unroll
+            for (int i = 0; i < G; i++) {
+                if (look[i] && (e[i] & kmask) == key[i]) {   // (an empty slot reads 0, which is no key)
+                    g[i].done = true; g[i].kcy = true; g[i].mlam = (u32)(e[i] >> lsh);
+                }
+            }
+        }
         // service: record every decided game, refill its slot
         bool any = false;
 #pragma unroll
@@ -445,13 +534,15 @@ __device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __res
         if (__any_sync(WAR_FULL_MASK, any)) {
 #pragma unroll
             for (int i = 0; i < G; i++) {
-                LGame<EXTRA>& x = g[i];
+                LGame<EXTRA, MEMO>& x = g[i];
                 if (x.done & (x.st == ST_ACTIVE)) {
                     const bool cy = x.kcy;
                     turns += x.rounds;
-                    const u32 lam = x.rounds - ((x.next - W) >> 1);
+                    const u32 lam = (MEMO && x.mlam) ? x.mlam : x.rounds - ((x.next - W) >> 1);
                     if (cy) {
                         cyc++;
+                        if (MEMO && memo != nullptr && x.mlam == 0u)   // found by Brent: store its landmarks
+                            memo_store_cycle<RULE>(memo, mbits, x.w1, x.w2, TV ? x.q + qshift : x.q, n, lam);
                         if (a.hbins) atomicAdd(&shh[lam < hb1 ? lam : hb1], 1u);
                         if (CANON && EXTRA && a.distinct) {
                             const u32 tstep = (x.next - W) >> 1;
@@ -513,13 +604,15 @@ __device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __res
     flush_hist(she, acc->endhist, WAR_EBINS);
 }
 
-// Dispatch: variant V selects the turn form (V & 1: multiply-add) and the record scheme (V & 2: latched);
-// the loop-shape tracker needs the immediate scheme.
+// Dispatch: variant V selects the turn form (V & 1: multiply-add), the record scheme (V & 2: latched)
+// and, for deals with the latched scheme, the cycle memo (V & 4); the loop-shape tracker needs the
+// immediate scheme.
 template <int RULE, int G, bool CANON, bool SHAPE, bool EXTRA, int V>
 __device__ __forceinline__ void refill_dispatch(const BatchArgs& a, DevAcc* __restrict__ acc, u64* __restrict__ counter,
                                                 u32* sh) {
     if constexpr (SHAPE || (V & 2) == 0) refill_body<RULE, G, CANON, SHAPE, EXTRA, V & 1>(a, acc, counter, sh);
-    else refill_latched<RULE, G, CANON, EXTRA, V & 1>(a, acc, counter, sh);
+    else if constexpr (!CANON && (V & 4) != 0) refill_latched<RULE, G, CANON, EXTRA, V & 1, true>(a, acc, counter, sh);
+    else refill_latched<RULE, G, CANON, EXTRA, V & 1, false>(a, acc, counter, sh);
 }
 
 }  // namespace war

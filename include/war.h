@@ -80,8 +80,11 @@ typedef struct war_tune {
     int32_t defer;         /* immediate records: lanes that wait, decided, before the warp refills them (1..32);
                               latched records: iterations between services (rounded up to a multiple of 4) */
     int32_t variant;       /* bit 0: multiply-add turn form (else logic/shift); bit 1: outcomes latched and
-                              recorded every `defer` iterations (else recorded at once); same results */
-    int32_t reserved;
+                              recorded every `defer` iterations (else recorded at once); bit 2 (deals with
+                              bit 1, n <= 15): cycle memo, a game is decided as soon as it passes a state of
+                              a cycle found before in the job (`turns` then counts the turns played, fewer
+                              than the reference's schedule); same results otherwise */
+    int32_t memo_bits;     /* cycle memo: log2 of its 8-byte slots (12..28); 0 = 24 (128 MiB) */
 } war_tune;
 
 /* Aggregates of one job.  Matches what gpu/war_gpu.py run() returns (gpu/war_gpu.py:346-352) before

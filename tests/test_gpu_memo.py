@@ -1,0 +1,84 @@
+"""The cycle memo (tune variant bit 2): deals decided at the first memoised landmark of their cycle give
+the same counts as Brent alone — whole a(12) and a(13), both rules, slices of n = 14 and 15 (where the
+cycle length field of a memo entry is narrowest), a table too small to hold the cycles, and the seeded
+sample aggregates."""
+import random
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("cyc", "done", "maxfin", "shape_nonstd", "shape_unchecked", "oncycle", "distinct_min", "s_count", "s_cyc",
+          "s_lamsum", "s_lensum", "s_maxfin")
+
+
+def memo_tune(wl, **kw):
+    t = dict(variant=7, games=2, threads=256, defer=8)
+    t.update(kw)
+    return wl.make_tune(**t)
+
+
+def same(wl, a, b):
+    da, db = wl.to_dict(a), wl.to_dict(b)
+    for k in FIELDS + ("hist", "dhist", "endhist"):
+        assert da[k] == db[k], (k, da[k], db[k])
+
+
+def test_memo_full_a12_a13(wl, golden):
+    for n in (12, 13):
+        r = wl.enumerate_job(wl.make_job(n, hbins=256), memo_tune(wl))
+        d = wl.to_dict(r)
+        g = golden["deals_rule0"][n]
+        assert (d["done"], d["cyc"], d["maxfin"], d["hist"]) == (g["deals"], g["cyc"], g["longest"], g["hist"])
+        assert max(d["endhist"]) == g["longest"]
+        base = wl.enumerate_job(wl.make_job(n, hbins=256), wl.make_tune(variant=3, games=2, threads=256, defer=8))
+        same(wl, r, base)
+        if n == 13:
+            assert r.turns < base.turns / 2   # the memo decides most cycling deals early
+
+
+def test_memo_rule1_a13(wl, golden):
+    r = wl.enumerate_job(wl.make_job(13, rule=1), memo_tune(wl, variant=6, games=1, threads=512))
+    g = golden["deals_rule1"][13]
+    assert (r.done, r.cyc, r.maxfin) == (g["deals"], g["cyc"], g["longest"])
+
+
+@pytest.mark.parametrize("bits", [12, 16])
+def test_memo_small_table(wl, bits):
+    """A table far smaller than the cycles' landmarks: inserts give up, lookups miss, counts stay exact."""
+    job = wl.make_job(12, lo=10 ** 8, hi=2 * 10 ** 8, hbins=128)
+    same(wl, wl.enumerate_job(job, memo_tune(wl, memo_bits=bits)), wl.enumerate_plain(job))
+
+
+@pytest.mark.parametrize("n,lo,span", [(14, 7 * 10 ** 9, 3 * 10 ** 8), (15, 10 ** 12, 2 * 10 ** 8),
+                                       (15, 3 * 10 ** 11 + 12345, 10 ** 7), (11, 0, 39916800)])
+def test_memo_slices_vs_plain(wl, n, lo, span):
+    for rule in (0, 1):
+        job = wl.make_job(n, rule=rule, lo=lo, hi=lo + span, hbins=512)
+        same(wl, wl.enumerate_job(job, memo_tune(wl)), wl.enumerate_plain(job))
+
+
+def test_memo_random_ranges_with_sample(wl, oracle):
+    rnd = random.Random(4242)
+    for n in (5, 7, 9, 10, 11):
+        total = wl.space_size(n, wl.DEALS)
+        for _ in range(3):
+            lo = rnd.randrange(0, total)
+            hi = min(total, lo + rnd.choice([1, 33, 5000, 400000]))
+            job = wl.make_job(n, rule=rnd.randint(0, 1), flags=wl.F_SAMPLE, sample_ppm=50000, seed=11, lo=lo, hi=hi,
+                              hbins=128)
+            want = oracle.enumerate_job(oracle.make_job(n, 0, job.rule, job.flags, lo, hi, 128, 0, 0, 50000, 11))
+            got = wl.to_dict(wl.enumerate_job(job, memo_tune(wl, games=rnd.choice([1, 2]))))
+            w = oracle.to_dict(want)
+            for k in FIELDS + ("hist", "endhist"):
+                assert got[k] == w[k], (n, lo, hi, k)
+
+
+def test_memo_ignored_where_it_does_not_apply(wl, oracle):
+    """Canonical scans, the immediate-record loop and n = 16 run without the memo, same counts."""
+    job = wl.make_job(10, wl.CANON, flags=wl.F_DISTINCT, hbins=64, dbins=64)
+    same(wl, wl.enumerate_job(job, memo_tune(wl)), wl.enumerate_job(job))
+    job = wl.make_job(11, hbins=64)
+    same(wl, wl.enumerate_job(job, wl.make_tune(variant=5)), wl.enumerate_job(job))
+    job = wl.make_job(16, lo=10 ** 13, hi=10 ** 13 + 2 * 10 ** 6, hbins=128)
+    same(wl, wl.enumerate_job(job, memo_tune(wl)), wl.enumerate_plain(job))
