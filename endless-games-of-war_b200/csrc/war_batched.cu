@@ -29,15 +29,19 @@ static BatchedFn pick_v(int canon, int rule, int shape, int extra, int games) {
     return games == 2 ? pick_g<0, 2, V>(canon, shape, extra) : pick_g<0, 1, V>(canon, shape, extra);
 }
 
-// variant: bit 0 = multiply-add turn form, bit 1 = latched records, bit 2 = cycle memo (deals, latched)
+// variant: bit 0 = multiply-add turn form, bit 1 = latched records, bit 2 = cycle memo (deals, latched),
+// bit 3 = the memo holds every cycle state (else landmarks)
 static BatchedFn pick(int canon, int rule, int shape, int extra, int games, int variant) {
     if (canon || (variant & 2) == 0) variant &= 3;
+    if ((variant & 4) == 0) variant &= 7;
     switch (variant) {
         case 1: return pick_v<1>(canon, rule, shape, extra, games);
         case 2: return pick_v<2>(canon, rule, shape, extra, games);
         case 3: return pick_v<3>(canon, rule, shape, extra, games);
         case 6: return pick_v<6>(canon, rule, shape, extra, games);
         case 7: return pick_v<7>(canon, rule, shape, extra, games);
+        case 14: return pick_v<14>(canon, rule, shape, extra, games);
+        case 15: return pick_v<15>(canon, rule, shape, extra, games);
         default: return pick_v<0>(canon, rule, shape, extra, games);
     }
 }

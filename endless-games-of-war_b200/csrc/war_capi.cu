@@ -51,7 +51,8 @@ int check_job(const war_job* j) {
     if (j->rule != 0 && j->rule != 1) return fail(WAR_EINVAL, "rule=%d", j->rule);
     if (j->hbins < 0 || j->hbins > WAR_HBINS_MAX) return fail(WAR_EINVAL, "hbins=%d outside 0..%d", j->hbins, WAR_HBINS_MAX);
     if (j->dbins < 0 || j->dbins > WAR_DBINS_MAX) return fail(WAR_EINVAL, "dbins=%d outside 0..%d", j->dbins, WAR_DBINS_MAX);
-    if (j->flags & ~(WAR_F_HALF | WAR_F_DISTINCT | WAR_F_SHAPE | WAR_F_SAMPLE)) return fail(WAR_EINVAL, "flags=0x%x", j->flags);
+    if (j->flags & ~(WAR_F_HALF | WAR_F_DISTINCT | WAR_F_SHAPE | WAR_F_SAMPLE | WAR_F_MEMO_KEEP))
+        return fail(WAR_EINVAL, "flags=0x%x", j->flags);
     if ((j->flags & WAR_F_HALF) && (j->mode != WAR_DEALS || (j->n & 1)))
         return fail(WAR_EINVAL, "WAR_F_HALF needs deals with even n");
     if (j->sample_ppm > 1000000u) return fail(WAR_EINVAL, "sample_ppm=%u above 10^6", j->sample_ppm);
@@ -206,10 +207,12 @@ int resolve_tune(const war_job* job, const war_tune* in, Tune& t) {
     if (t.block_m < 1 || t.block_m > 8) return fail(WAR_EINVAL, "tune.block_m=%d (1..8)", t.block_m);
     if (t.window < 1 || t.window > (1 << 16) || (t.window & (t.window - 1))) return fail(WAR_EINVAL, "tune.window=%d", t.window);
     if (t.defer < 1 || t.defer > 32) return fail(WAR_EINVAL, "tune.defer=%d (1..32)", t.defer);
-    if (t.variant < 0 || t.variant > 7) return fail(WAR_EINVAL, "tune.variant=%d (0..7)", t.variant);
+    if (t.variant < 0 || t.variant > 15) return fail(WAR_EINVAL, "tune.variant=%d (0..15)", t.variant);
     if (t.memo_bits < 12 || t.memo_bits > 28) return fail(WAR_EINVAL, "tune.memo_bits=%d (12..28)", t.memo_bits);
-    // the cycle memo serves deals of 4..15 cards with latched records
+    // the cycle memo serves deals of 4..15 cards with latched records; all states up to 14 cards
     if ((t.variant & 4) && (canon || !(t.variant & 2) || job->n < 4 || job->n > 15)) t.variant &= 3;
+    if ((t.variant & 8) && job->n > 14) t.variant &= 7;
+    if (!(t.variant & 4)) t.variant &= 7;
     const int M = canon ? job->n - 1 : job->n;
     if (t.block_m > M) t.block_m = M > 0 ? M : 1;
     int st = ensure_ready();
@@ -499,8 +502,10 @@ int war_enumerate(const war_job* job, const war_tune* tune, war_result* out) {
     a.seed = job->seed;
     a.thr = ((u64)job->sample_ppm << 32) / 1000000u;
     a.units = c.d_units;
-    if (t.variant & 4) {   // the cycle memo, cleared for this job
+    if (t.variant & 4) {   // the cycle memo: cleared for this job unless kept from the last one of this n and rule
         const size_t bytes = sizeof(u64) << t.memo_bits;
+        const bool keep = (job->flags & WAR_F_MEMO_KEEP) && c.memo_bits == t.memo_bits && c.memo_n == job->n &&
+                          c.memo_rule == job->rule;
         if (c.memo_bits != t.memo_bits) {
             if (c.d_memo) cudaFree(c.d_memo);
             c.d_memo = nullptr;
@@ -511,8 +516,12 @@ int war_enumerate(const war_job* job, const war_tune* tune, war_result* out) {
             }
             c.memo_bits = t.memo_bits;
         }
-        if ((e = cudaMemsetAsync(c.d_memo, 0, bytes, cur_stream())) != cudaSuccess)
+        if (!keep && (e = cudaMemsetAsync(c.d_memo, 0, bytes, cur_stream())) != cudaSuccess) {
+            c.memo_n = -1;
             return cuda_fail(e, "clear cycle memo");
+        }
+        c.memo_n = job->n;
+        c.memo_rule = job->rule;
         a.memo = c.d_memo;
         a.memo_bits = (u32)t.memo_bits;
     }

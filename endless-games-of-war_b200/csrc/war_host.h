@@ -20,6 +20,7 @@ struct Ctx {
     size_t sample_cap = 0;
     u64* d_memo = nullptr;          // cycle memo table of the refill kernel (deals)
     int memo_bits = 0;
+    int memo_n = -1, memo_rule = -1;  // job class whose cycles the memo holds
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 

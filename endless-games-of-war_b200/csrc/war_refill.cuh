@@ -388,15 +388,36 @@ __device__ __forceinline__ void memo_put(u64* T, u32 bits, u64 key, u32 lsh, u32
     if (__ldcg(p) < val) atomicMax(p, val);
 }
 
-// Walks the cycle of length lam through the state (w1, w2, q4 = 4*len1) once and stores its landmarks.
-template <int RULE>
+// The all-states memo (MEMO_ALL) holds every state of a found cycle instead of its landmarks, so a game
+// is looked up at its current state and needs nothing kept per turn.  Entry: the pile that is smaller as
+// a 64-bit word first (either orientation gives the same key), its cards then the other pile's as 4(n-1)
+// bits of nibbles (the last card is the one missing), its length in 4 bits, the cycle length in the top
+// 64 - 4n bits.  n <= 14.
+enum { MEMO_NONE = 0, MEMO_LANDMARK = 1, MEMO_ALL = 2 };
+
+__device__ __forceinline__ u64 memo_key_state(u64 w1, u64 w2, u32 n) {
+    const bool sw = w2 < w1;
+    const u64 h = sw ? w2 : w1, o = sw ? w1 : w2;
+    const u32 lh = pile_len(h);
+    const u64 cat = (h ^ (1ull << (4u * lh))) | (o << (4u * lh));
+    const u32 kb = 4u * (n - 1u);
+    return (cat & ((1ull << kb) - 1ull)) | ((u64)lh << kb);
+}
+
+template <int MODE>
+__device__ __forceinline__ u32 memo_lam_shift(u32 n) { return MODE == MEMO_ALL ? 4u * n : 4u * (n - 1u); }
+
+// Walks the cycle of length lam through the state (w1, w2, q4 = 4*len1) once and stores its landmarks
+// (MEMO_LANDMARK) or all its states (MEMO_ALL).
+template <int RULE, int MODE>
 __device__ __noinline__ void memo_store_cycle(u64* T, u32 bits, u64 w1, u64 w2, u32 q4, u32 n, u32 lam) {
-    const u32 lsh = 4u * (n - 1u);
+    const u32 lsh = memo_lam_shift<MODE>(n);
     if (lam == 0u || (u64)lam >> (64u - lsh) != 0ull) return;
     const u32 k4m4 = 4u * (n - 1u);
     const u64 top = (u64)(n - 1u);
     for (u32 t = 0; t < lam; t++) {
-        if ((w1 & 15ull) == top) memo_put(T, bits, memo_key(w1, w2, n), lsh, lam);
+        if (MODE == MEMO_ALL) memo_put(T, bits, memo_key_state(w1, w2, n), lsh, lam);
+        else if ((w1 & 15ull) == top) memo_put(T, bits, memo_key(w1, w2, n), lsh, lam);
         else if ((w2 & 15ull) == top) memo_put(T, bits, memo_key(w2, w1, n), lsh, lam);
         war_turn<RULE>(w1, w2, q4, k4m4);
     }
@@ -409,7 +430,7 @@ __device__ __noinline__ void memo_store_cycle(u64* T, u32 bits, u64 w1, u64 w2, 
 // slots: each done game is recorded and replaced by the lane's next position.  The record and refill
 // code therefore runs once per K iterations with every lane that has a done game, instead of once per
 // decided game with one lane.  The cycle test compares all four words (no candidate to verify later).
-template <bool EXTRA, bool MEMO>
+template <bool EXTRA, int MEMO>
 struct LGame {
     u64 w1, w2, t1, t2;
     u32 q, rounds, next, st;
@@ -419,10 +440,10 @@ struct LGame {
     u32 mlam;           // MEMO: cycle length given by the memo (0: decided by Brent)
 };
 
-// With MEMO, each turn also keeps the state before it when card n-1 is on top (a landmark), and every
-// service looks the kept landmark of each undecided game up in the memo; a game decided by Brent stores
-// its cycle's landmarks.
-template <int RULE, int G, bool CANON, bool EXTRA, int TV, bool MEMO>
+// With MEMO_LANDMARK, each turn also keeps the state before it when card n-1 is on top (a landmark), and
+// every service looks the kept landmark of each undecided game up in the memo; with MEMO_ALL every
+// service looks up each undecided game's current state.  A game decided by Brent stores its cycle.
+template <int RULE, int G, bool CANON, bool EXTRA, int TV, int MEMO>
 __device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __restrict__ acc, u64* __restrict__ counter,
                                                u32* sh) {
     u32* shh = sh;
@@ -448,7 +469,7 @@ __device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __res
     u32 sc = 0, scy = 0, slam = 0, slen = 0, smax = 0, oncyc = 0, dmin = 0;
     const u32 nm1 = n - 1u;
     u64* const memo = MEMO ? a.memo : nullptr;
-    const u32 mbits = a.memo_bits, lsh = 4u * (n - 1u);
+    const u32 mbits = a.memo_bits, lsh = memo_lam_shift<MEMO>(n);
     const u64 kmask = lsh < 64u ? (1ull << lsh) - 1ull : ~0ull;
 
     auto start_game = [&](LGame<EXTRA, MEMO>& x) {
@@ -479,7 +500,7 @@ __device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __res
 #pragma unroll
                 for (int i = 0; i < G; i++) {
                     LGame<EXTRA, MEMO>& x = g[i];
-                    if (MEMO) {
+                    if (MEMO == MEMO_LANDMARK) {
                         const u32 c1 = (u32)x.w1 & 15u, c2 = (u32)x.w2 & 15u;
                         const bool lm = max(c1, c2) == nm1;
                         x.m1 = lm ? x.w1 : x.m1;
@@ -514,11 +535,16 @@ __device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __res
 #pragma unroll
             for (int i = 0; i < G; i++) {
                 LGame<EXTRA, MEMO>& x = g[i];
-                look[i] = !x.done & (x.m1 != 0ull);
-                const bool h1 = ((u32)x.m1 & 15u) == nm1;
-                key[i] = memo_key(h1 ? x.m1 : x.m2, h1 ? x.m2 : x.m1, n);
+                if (MEMO == MEMO_ALL) {
+                    look[i] = !x.done;
+                    key[i] = memo_key_state(x.w1, x.w2, n);
+                } else {
+                    look[i] = !x.done & (x.m1 != 0ull);
+                    const bool h1 = ((u32)x.m1 & 15u) == nm1;
+                    key[i] = memo_key(h1 ? x.m1 : x.m2, h1 ? x.m2 : x.m1, n);
+                    x.m1 = 0ull;
+                }
                 e[i] = look[i] ? __ldcg((const unsigned long long*)memo + memo_slot(key[i], mbits)) : 0ull;
-                x.m1 = 0ull;
             }
 #pragma unroll
             for (int i = 0; i < G; i++) {
@@ -542,7 +568,7 @@ __device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __res
                     if (cy) {
                         cyc++;
                         if (MEMO && memo != nullptr && x.mlam == 0u)   // found by Brent: store its landmarks
-                            memo_store_cycle<RULE>(memo, mbits, x.w1, x.w2, TV ? x.q + qshift : x.q, n, lam);
+                            memo_store_cycle<RULE, MEMO>(memo, mbits, x.w1, x.w2, TV ? x.q + qshift : x.q, n, lam);
                         if (a.hbins) atomicAdd(&shh[lam < hb1 ? lam : hb1], 1u);
                         if (CANON && EXTRA && a.distinct) {
                             const u32 tstep = (x.next - W) >> 1;
@@ -605,14 +631,15 @@ __device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __res
 }
 
 // Dispatch: variant V selects the turn form (V & 1: multiply-add), the record scheme (V & 2: latched)
-// and, for deals with the latched scheme, the cycle memo (V & 4); the loop-shape tracker needs the
-// immediate scheme.
+// and, for deals with the latched scheme, the cycle memo (V & 4: landmarks, V & 12: all states); the
+// loop-shape tracker needs the immediate scheme.
 template <int RULE, int G, bool CANON, bool SHAPE, bool EXTRA, int V>
 __device__ __forceinline__ void refill_dispatch(const BatchArgs& a, DevAcc* __restrict__ acc, u64* __restrict__ counter,
                                                 u32* sh) {
     if constexpr (SHAPE || (V & 2) == 0) refill_body<RULE, G, CANON, SHAPE, EXTRA, V & 1>(a, acc, counter, sh);
-    else if constexpr (!CANON && (V & 4) != 0) refill_latched<RULE, G, CANON, EXTRA, V & 1, true>(a, acc, counter, sh);
-    else refill_latched<RULE, G, CANON, EXTRA, V & 1, false>(a, acc, counter, sh);
+    else if constexpr (CANON || (V & 4) == 0) refill_latched<RULE, G, CANON, EXTRA, V & 1, MEMO_NONE>(a, acc, counter, sh);
+    else if constexpr ((V & 8) != 0) refill_latched<RULE, G, CANON, EXTRA, V & 1, MEMO_ALL>(a, acc, counter, sh);
+    else refill_latched<RULE, G, CANON, EXTRA, V & 1, MEMO_LANDMARK>(a, acc, counter, sh);
 }
 
 }  // namespace war

@@ -14,7 +14,7 @@ WAR_HBINS_MAX = 4096
 WAR_DBINS_MAX = 4096
 WAR_EBINS = 1024
 DEALS, CANON = 0, 1
-F_HALF, F_DISTINCT, F_SHAPE, F_SAMPLE = 1, 2, 4, 8
+F_HALF, F_DISTINCT, F_SHAPE, F_SAMPLE, F_MEMO_KEEP = 1, 2, 4, 8, 16
 
 STATUS = {0: "ok", -1: "invalid argument", -2: "CUDA error", -3: "timeout", -4: "out of memory",
           -5: "busy", -6: "not found", -7: "turn cap exceeded", -8: "no CUDA device", 1: "pending"}

@@ -49,7 +49,11 @@ enum war_flags {
     WAR_F_HALF = 1,     /* even n, deals: play only deals that give card n-1 to player 1 (gpu/war_gpu.py:147-154) */
     WAR_F_DISTINCT = 2, /* canon: distinct-cycle weights + min-key count (gpu/war_gpu.py:217-235, cpu/distinct_cycles.c:67-80) */
     WAR_F_SHAPE = 4,    /* canon: Theorem-3 loop-shape test, blk = n & -n (gpu/war_gpu.py:51-73, :290) */
-    WAR_F_SAMPLE = 8    /* accumulate the seeded sample aggregates used by the Floyd cross-check */
+    WAR_F_SAMPLE = 8,   /* accumulate the seeded sample aggregates used by the Floyd cross-check */
+    WAR_F_MEMO_KEEP = 16 /* deals with the cycle memo (war_tune.variant bit 2): start from the memo left by the
+                            previous war_enumerate of the same n and rule instead of an empty one (its entries
+                            are facts about n and the rule, not about the range); no other effect (no
+                            reference counterpart) */
 };
 
 /* One enumeration job: the ranks [lo, hi) of one space.
@@ -83,7 +87,9 @@ typedef struct war_tune {
                               recorded every `defer` iterations (else recorded at once); bit 2 (deals with
                               bit 1, n <= 15): cycle memo, a game is decided as soon as it passes a state of
                               a cycle found before in the job (`turns` then counts the turns played, fewer
-                              than the reference's schedule); same results otherwise */
+                              than the reference's schedule); bit 3 (with bit 2, n <= 14): the memo holds
+                              every state of the found cycles and games are looked up at their current
+                              state (else cycle landmarks, kept per turn); same results otherwise */
     int32_t memo_bits;     /* cycle memo: log2 of its 8-byte slots (12..28); 0 = 24 (128 MiB) */
 } war_tune;
 

@@ -1,5 +1,5 @@
-"""The cycle memo (tune variant bit 2): deals decided at the first memoised landmark of their cycle give
-the same counts as Brent alone — whole a(12) and a(13), both rules, slices of n = 14 and 15 (where the
+"""The cycle memo (tune variant bit 2, landmarks; with bit 3, every cycle state): deals decided as soon as
+they meet a memoised state of their cycle give the same counts as Brent alone — whole a(12) and a(13), both rules, slices of n = 14 and 15 (where the
 cycle length field of a memo entry is narrowest), a table too small to hold the cycles, and the seeded
 sample aggregates."""
 import random
@@ -24,9 +24,10 @@ def same(wl, a, b):
         assert da[k] == db[k], (k, da[k], db[k])
 
 
-def test_memo_full_a12_a13(wl, golden):
+@pytest.mark.parametrize("variant", [7, 15])
+def test_memo_full_a12_a13(wl, golden, variant):
     for n in (12, 13):
-        r = wl.enumerate_job(wl.make_job(n, hbins=256), memo_tune(wl))
+        r = wl.enumerate_job(wl.make_job(n, hbins=256), memo_tune(wl, variant=variant))
         d = wl.to_dict(r)
         g = golden["deals_rule0"][n]
         assert (d["done"], d["cyc"], d["maxfin"], d["hist"]) == (g["deals"], g["cyc"], g["longest"], g["hist"])
@@ -43,11 +44,11 @@ def test_memo_rule1_a13(wl, golden):
     assert (r.done, r.cyc, r.maxfin) == (g["deals"], g["cyc"], g["longest"])
 
 
-@pytest.mark.parametrize("bits", [12, 16])
-def test_memo_small_table(wl, bits):
-    """A table far smaller than the cycles' landmarks: inserts give up, lookups miss, counts stay exact."""
+@pytest.mark.parametrize("bits,variant", [(12, 7), (16, 7), (12, 15), (16, 14)])
+def test_memo_small_table(wl, bits, variant):
+    """A table far smaller than the cycles' states: most inserts are lost, lookups miss, counts stay exact."""
     job = wl.make_job(12, lo=10 ** 8, hi=2 * 10 ** 8, hbins=128)
-    same(wl, wl.enumerate_job(job, memo_tune(wl, memo_bits=bits)), wl.enumerate_plain(job))
+    same(wl, wl.enumerate_job(job, memo_tune(wl, memo_bits=bits, variant=variant)), wl.enumerate_plain(job))
 
 
 @pytest.mark.parametrize("n,lo,span", [(14, 7 * 10 ** 9, 3 * 10 ** 8), (15, 10 ** 12, 2 * 10 ** 8),
@@ -55,7 +56,9 @@ def test_memo_small_table(wl, bits):
 def test_memo_slices_vs_plain(wl, n, lo, span):
     for rule in (0, 1):
         job = wl.make_job(n, rule=rule, lo=lo, hi=lo + span, hbins=512)
-        same(wl, wl.enumerate_job(job, memo_tune(wl)), wl.enumerate_plain(job))
+        plain = wl.enumerate_plain(job)
+        same(wl, wl.enumerate_job(job, memo_tune(wl)), plain)
+        same(wl, wl.enumerate_job(job, memo_tune(wl, variant=15, games=1)), plain)   # all states (n <= 14)
 
 
 def test_memo_random_ranges_with_sample(wl, oracle):
@@ -68,7 +71,8 @@ def test_memo_random_ranges_with_sample(wl, oracle):
             job = wl.make_job(n, rule=rnd.randint(0, 1), flags=wl.F_SAMPLE, sample_ppm=50000, seed=11, lo=lo, hi=hi,
                               hbins=128)
             want = oracle.enumerate_job(oracle.make_job(n, 0, job.rule, job.flags, lo, hi, 128, 0, 0, 50000, 11))
-            got = wl.to_dict(wl.enumerate_job(job, memo_tune(wl, games=rnd.choice([1, 2]))))
+            got = wl.to_dict(wl.enumerate_job(job, memo_tune(wl, games=rnd.choice([1, 2]),
+                                                             variant=rnd.choice([6, 7, 14, 15]))))
             w = oracle.to_dict(want)
             for k in FIELDS + ("hist", "endhist"):
                 assert got[k] == w[k], (n, lo, hi, k)
@@ -82,3 +86,20 @@ def test_memo_ignored_where_it_does_not_apply(wl, oracle):
     same(wl, wl.enumerate_job(job, wl.make_tune(variant=5)), wl.enumerate_job(job))
     job = wl.make_job(16, lo=10 ** 13, hi=10 ** 13 + 2 * 10 ** 6, hbins=128)
     same(wl, wl.enumerate_job(job, memo_tune(wl)), wl.enumerate_plain(job))
+
+
+def test_memo_kept_across_jobs(wl):
+    """WAR_F_MEMO_KEEP: a job that starts from the memo of the previous job of the same n and rule counts the
+    same; a kept memo of another n or rule is not used (the job clears it)."""
+    t = memo_tune(wl, variant=15)
+    a = wl.make_job(13, lo=10 ** 9, hi=10 ** 9 + 3 * 10 ** 8, hbins=128)
+    b = wl.make_job(13, flags=wl.F_MEMO_KEEP, lo=4 * 10 ** 9, hi=4 * 10 ** 9 + 3 * 10 ** 8, hbins=128)
+    cold = wl.enumerate_job(b, wl.make_tune(variant=3, games=2, threads=256, defer=8))
+    wl.enumerate_job(a, t)
+    warm = wl.enumerate_job(b, t)
+    same(wl, warm, cold)
+    assert warm.turns < cold.turns
+    wl.enumerate_job(wl.make_job(12, rule=1, lo=0, hi=10 ** 8), t)
+    same(wl, wl.enumerate_job(b, t), cold)   # the rule-1 n = 12 memo is not kept for n = 13 rule 0
+    c = wl.make_job(12, flags=wl.F_MEMO_KEEP, lo=2 * 10 ** 8, hi=4 * 10 ** 8, hbins=128)
+    same(wl, wl.enumerate_job(c, t), wl.enumerate_plain(wl.make_job(12, lo=2 * 10 ** 8, hi=4 * 10 ** 8, hbins=128)))
