@@ -10,7 +10,7 @@ at a time, over
     window         Brent's first tortoise window                         (8..128)
     defer          lanes that wait, decided, before the warp refills     (1..8)
     variant        bit 0: multiply-add turn form; bit 1: latched records serviced every `defer` iterations;
-                   bit 2: cycle memo (deals); bit 3: the memo holds every cycle state
+                   bit 2: cycle memo (deals); bit 3: the memo holds every cycle state; bit 4: and paths
 Every configuration must return exactly the same counts as the first one; a mismatch raises.  The best
 configuration is stored in tune_cache.json next to this file, keyed by GPU name, n, mode, rule and flags.
 
@@ -35,7 +35,7 @@ SPACE = {
     "blocks_per_sm": [0, 1, 2, 3, 4],
     "window": [8, 16, 32, 64, 128],
     "defer": [1, 2, 4, 6, 8, 12, 16, 24, 32],
-    "variant": [0, 1, 2, 3, 6, 7, 14, 15],
+    "variant": [0, 1, 2, 3, 6, 7, 14, 15, 30, 31],
     "memo_bits": [24, 25, 26, 27, 28],
 }
 DEFAULT = {"block_m": 5, "games": 2, "threads": 512, "blocks_per_sm": 0, "window": 32, "defer": 8, "variant": 1,

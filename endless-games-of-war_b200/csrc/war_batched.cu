@@ -30,10 +30,11 @@ static BatchedFn pick_v(int canon, int rule, int shape, int extra, int games) {
 }
 
 // variant: bit 0 = multiply-add turn form, bit 1 = latched records, bit 2 = cycle memo (deals, latched),
-// bit 3 = the memo holds every cycle state (else landmarks)
+// bit 3 = the memo holds every cycle state (else landmarks), bit 4 = and the paths of decided games
 static BatchedFn pick(int canon, int rule, int shape, int extra, int games, int variant) {
     if (canon || (variant & 2) == 0) variant &= 3;
     if ((variant & 4) == 0) variant &= 7;
+    if ((variant & 8) == 0) variant &= 15;
     switch (variant) {
         case 1: return pick_v<1>(canon, rule, shape, extra, games);
         case 2: return pick_v<2>(canon, rule, shape, extra, games);
@@ -42,6 +43,8 @@ static BatchedFn pick(int canon, int rule, int shape, int extra, int games, int 
         case 7: return pick_v<7>(canon, rule, shape, extra, games);
         case 14: return pick_v<14>(canon, rule, shape, extra, games);
         case 15: return pick_v<15>(canon, rule, shape, extra, games);
+        case 30: return pick_v<30>(canon, rule, shape, extra, games);
+        case 31: return pick_v<31>(canon, rule, shape, extra, games);
         default: return pick_v<0>(canon, rule, shape, extra, games);
     }
 }

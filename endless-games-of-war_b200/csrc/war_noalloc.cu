@@ -144,7 +144,7 @@ extern "C" int war_enumerate_noalloc(const war_job* job, const war_tune* tune, w
     if (block_m < 1 || block_m > 8) return fail(WAR_EINVAL, "tune.block_m=%d (1..8)", block_m);
     if (window < 1 || window > (1 << 16) || (window & (window - 1))) return fail(WAR_EINVAL, "tune.window=%d", window);
     if (defer < 1 || defer > 32) return fail(WAR_EINVAL, "tune.defer=%d (1..32)", defer);
-    if (variant < 0 || variant > 15) return fail(WAR_EINVAL, "tune.variant=%d (0..15)", variant);
+    if (variant < 0 || variant > 31) return fail(WAR_EINVAL, "tune.variant=%d (0..31)", variant);
     variant &= 3;   // no cycle memo: its table would be allocated memory
     if (block_m > M) block_m = M > 0 ? M : 1;
 

@@ -393,7 +393,13 @@ __device__ __forceinline__ void memo_put(u64* T, u32 bits, u64 key, u32 lsh, u32
 // a 64-bit word first (either orientation gives the same key), its cards then the other pile's as 4(n-1)
 // bits of nibbles (the last card is the one missing), its length in 4 bits, the cycle length in the top
 // 64 - 4n bits.  n <= 14.
-enum { MEMO_NONE = 0, MEMO_LANDMARK = 1, MEMO_ALL = 2 };
+//
+// The path memo (MEMO_PATH) adds, for every decided game, the states at which it was looked up and
+// missed (the last two), with the game's outcome from there: "on a cycle of length lam" (value 2 lam) or
+// "ends after r more turns" (value 2r + 1).  Deals of nearby ranks often merge into one another's paths
+// after a few turns, so a later game is decided where it meets such a state.  Path entries are plain
+// stores that overwrite the slot (the most recent paths are the useful ones).
+enum { MEMO_NONE = 0, MEMO_LANDMARK = 1, MEMO_ALL = 2, MEMO_PATH = 3 };
 
 __device__ __forceinline__ u64 memo_key_state(u64 w1, u64 w2, u32 n) {
     const bool sw = w2 < w1;
@@ -405,18 +411,23 @@ __device__ __forceinline__ u64 memo_key_state(u64 w1, u64 w2, u32 n) {
 }
 
 template <int MODE>
-__device__ __forceinline__ u32 memo_lam_shift(u32 n) { return MODE == MEMO_ALL ? 4u * n : 4u * (n - 1u); }
+__device__ __forceinline__ u32 memo_lam_shift(u32 n) { return MODE >= MEMO_ALL ? 4u * n : 4u * (n - 1u); }
 
 // Walks the cycle of length lam through the state (w1, w2, q4 = 4*len1) once and stores its landmarks
-// (MEMO_LANDMARK) or all its states (MEMO_ALL).
+// (MEMO_LANDMARK) or all its states (MEMO_ALL, MEMO_PATH).
 template <int RULE, int MODE>
 __device__ __noinline__ void memo_store_cycle(u64* T, u32 bits, u64 w1, u64 w2, u32 q4, u32 n, u32 lam) {
     const u32 lsh = memo_lam_shift<MODE>(n);
-    if (lam == 0u || (u64)lam >> (64u - lsh) != 0ull) return;
+    const u32 v = MODE == MEMO_PATH ? 2u * lam : lam;
+    if (lam == 0u || (u64)v >> (64u - lsh) != 0ull) return;
     const u32 k4m4 = 4u * (n - 1u);
     const u64 top = (u64)(n - 1u);
     for (u32 t = 0; t < lam; t++) {
-        if (MODE == MEMO_ALL) memo_put(T, bits, memo_key_state(w1, w2, n), lsh, lam);
+        if (MODE == MEMO_PATH) {
+            unsigned long long* p = (unsigned long long*)T + memo_slot(memo_key_state(w1, w2, n), bits);
+            const unsigned long long val = memo_key_state(w1, w2, n) | ((u64)v << lsh);
+            if (__ldcg(p) != val) __stcg(p, val);
+        } else if (MODE == MEMO_ALL) memo_put(T, bits, memo_key_state(w1, w2, n), lsh, lam);
         else if ((w1 & 15ull) == top) memo_put(T, bits, memo_key(w1, w2, n), lsh, lam);
         else if ((w2 & 15ull) == top) memo_put(T, bits, memo_key(w2, w1, n), lsh, lam);
         war_turn<RULE>(w1, w2, q4, k4m4);
@@ -436,8 +447,10 @@ struct LGame {
     u32 q, rounds, next, st;
     bool done, kcy;     // decided; decided by a cycle (else by an end)
     u64 s1, s2; u32 sq; bool sampled;
-    u64 m1, m2;         // MEMO: the last landmark passed since the last lookup (m1 = 0: none)
-    u32 mlam;           // MEMO: cycle length given by the memo (0: decided by Brent)
+    u64 m1, m2;         // MEMO_LANDMARK: the last landmark passed since the last lookup (m1 = 0: none)
+    u32 mlam;           // MEMO: the memo's value for this game (0: decided by Brent or by its end)
+    u64 pa1, pa2, pb1, pb2;   // MEMO_PATH: the last two states looked up and missed,
+    u32 ta, tb;               // at these turns (0: none)
 };
 
 // With MEMO_LANDMARK, each turn also keeps the state before it when card n-1 is on top (a landmark), and
@@ -479,6 +492,7 @@ __device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __res
         x.t1 = x.w1; x.t2 = x.w2; x.rounds = 0; x.next = W;
         x.done = !ok; x.kcy = false;
         if (MEMO) { x.m1 = 0ull; x.m2 = 0ull; x.mlam = 0u; }
+        if (MEMO == MEMO_PATH) { x.ta = 0u; x.tb = 0u; }
         if (EXTRA) {
             x.s1 = x.w1; x.s2 = x.w2; x.sq = x.q;
             x.sampled = a.sample && ok && war_pick(a.seed, a.thr, x.w1, x.w2);
@@ -535,7 +549,7 @@ __device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __res
 #pragma unroll
             for (int i = 0; i < G; i++) {
                 LGame<EXTRA, MEMO>& x = g[i];
-                if (MEMO == MEMO_ALL) {
+                if (MEMO >= MEMO_ALL) {
                     look[i] = !x.done;
                     key[i] = memo_key_state(x.w1, x.w2, n);
                 } else {
@@ -548,8 +562,13 @@ __device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __res
             }
 #pragma unroll
             for (int i = 0; i < G; i++) {
+                LGame<EXTRA, MEMO>& x = g[i];
                 if (look[i] && (e[i] & kmask) == key[i]) {   // (an empty slot reads 0, which is no key)
-                    g[i].done = true; g[i].kcy = true; g[i].mlam = (u32)(e[i] >> lsh);
+                    const u32 v = (u32)(e[i] >> lsh);
+                    x.done = true; x.kcy = MEMO == MEMO_PATH ? (v & 1u) == 0u : true; x.mlam = v;
+                } else if (MEMO == MEMO_PATH && look[i]) {
+                    x.pb1 = x.pa1; x.pb2 = x.pa2; x.tb = x.ta;
+                    x.pa1 = x.w1; x.pa2 = x.w2; x.ta = x.rounds;
                 }
             }
         }
@@ -564,10 +583,26 @@ __device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __res
                 if (x.done & (x.st == ST_ACTIVE)) {
                     const bool cy = x.kcy;
                     turns += x.rounds;
-                    const u32 lam = (MEMO && x.mlam) ? x.mlam : x.rounds - ((x.next - W) >> 1);
+                    // the memo's cycle length, or (path memo) the turns left after the memoised state
+                    const u32 mcy = MEMO == MEMO_PATH ? (x.mlam & 1u ? 0u : x.mlam >> 1) : x.mlam;
+                    const u32 len = MEMO == MEMO_PATH && (x.mlam & 1u) ? x.rounds + (x.mlam >> 1) : x.rounds;
+                    const u32 lam = (MEMO && mcy) ? mcy : x.rounds - ((x.next - W) >> 1);
+                    if (MEMO == MEMO_PATH && memo != nullptr) {   // the states it missed, with its outcome
+                        const u64 vmax = 1ull << (64u - lsh);
+                        if (x.ta) {
+                            const u64 v = cy ? 2ull * lam : 2ull * (len - x.ta) + 1ull;
+                            const u64 k = memo_key_state(x.pa1, x.pa2, n);
+                            if (v < vmax) __stcg((unsigned long long*)memo + memo_slot(k, mbits), k | (v << lsh));
+                        }
+                        if (x.tb) {
+                            const u64 v = cy ? 2ull * lam : 2ull * (len - x.tb) + 1ull;
+                            const u64 k = memo_key_state(x.pb1, x.pb2, n);
+                            if (v < vmax) __stcg((unsigned long long*)memo + memo_slot(k, mbits), k | (v << lsh));
+                        }
+                    }
                     if (cy) {
                         cyc++;
-                        if (MEMO && memo != nullptr && x.mlam == 0u)   // found by Brent: store its landmarks
+                        if (MEMO && memo != nullptr && mcy == 0u)   // found by Brent: store its cycle
                             memo_store_cycle<RULE, MEMO>(memo, mbits, x.w1, x.w2, TV ? x.q + qshift : x.q, n, lam);
                         if (a.hbins) atomicAdd(&shh[lam < hb1 ? lam : hb1], 1u);
                         if (CANON && EXTRA && a.distinct) {
@@ -586,13 +621,13 @@ __device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __res
                             }
                         }
                     } else {
-                        if (x.rounds > maxfin) maxfin = x.rounds;
-                        atomicAdd(&she[x.rounds < WAR_EBINS - 1 ? x.rounds : WAR_EBINS - 1], 1u);
+                        if (len > maxfin) maxfin = len;
+                        atomicAdd(&she[len < WAR_EBINS - 1 ? len : WAR_EBINS - 1], 1u);
                     }
                     if (EXTRA && x.sampled) {
                         sc++;
                         if (cy) { scy++; slam += lam; }
-                        else { slen += x.rounds; if (x.rounds > smax) smax = x.rounds; }
+                        else { slen += len; if (len > smax) smax = len; }
                     }
                 }
                 if (x.done & (x.st != ST_RETIRED)) start_game(x);
@@ -631,13 +666,14 @@ __device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __res
 }
 
 // Dispatch: variant V selects the turn form (V & 1: multiply-add), the record scheme (V & 2: latched)
-// and, for deals with the latched scheme, the cycle memo (V & 4: landmarks, V & 12: all states); the
-// loop-shape tracker needs the immediate scheme.
+// and, for deals with the latched scheme, the cycle memo (V & 4: landmarks, V & 12: all states, V & 28:
+// all states and paths); the loop-shape tracker needs the immediate scheme.
 template <int RULE, int G, bool CANON, bool SHAPE, bool EXTRA, int V>
 __device__ __forceinline__ void refill_dispatch(const BatchArgs& a, DevAcc* __restrict__ acc, u64* __restrict__ counter,
                                                 u32* sh) {
     if constexpr (SHAPE || (V & 2) == 0) refill_body<RULE, G, CANON, SHAPE, EXTRA, V & 1>(a, acc, counter, sh);
     else if constexpr (CANON || (V & 4) == 0) refill_latched<RULE, G, CANON, EXTRA, V & 1, MEMO_NONE>(a, acc, counter, sh);
+    else if constexpr ((V & 24) == 24) refill_latched<RULE, G, CANON, EXTRA, V & 1, MEMO_PATH>(a, acc, counter, sh);
     else if constexpr ((V & 8) != 0) refill_latched<RULE, G, CANON, EXTRA, V & 1, MEMO_ALL>(a, acc, counter, sh);
     else refill_latched<RULE, G, CANON, EXTRA, V & 1, MEMO_LANDMARK>(a, acc, counter, sh);
 }

@@ -89,8 +89,11 @@ typedef struct war_tune {
                               a cycle found before in the job (`turns` then counts the turns played, fewer
                               than the reference's schedule); bit 3 (with bit 2, n <= 14): the memo holds
                               every state of the found cycles and games are looked up at their current
-                              state (else cycle landmarks, kept per turn); same results otherwise */
-    int32_t memo_bits;     /* cycle memo: log2 of its 8-byte slots (12..28); 0 = 24 (128 MiB) */
+                              state (else cycle landmarks, kept per turn); bit 4 (with bits 2 and 3): the
+                              memo also holds states on the paths of decided games with their outcome
+                              (cycle length or turns left), so games that merge into an earlier game's path
+                              are decided there; same results otherwise */
+    int32_t memo_bits;     /* cycle memo: log2 of its 8-byte slots (12..31); 0 = 24 (128 MiB) */
 } war_tune;
 
 /* Aggregates of one job.  Matches what gpu/war_gpu.py run() returns (gpu/war_gpu.py:346-352) before

@@ -1,5 +1,6 @@
-"""The cycle memo (tune variant bit 2, landmarks; with bit 3, every cycle state): deals decided as soon as
-they meet a memoised state of their cycle give the same counts as Brent alone — whole a(12) and a(13), both rules, slices of n = 14 and 15 (where the
+"""The cycle memo (tune variant bit 2, landmarks; with bit 3, every cycle state; with bit 4, also states on
+the paths of decided games with their outcome): deals decided as soon as they meet a memoised state give
+the same counts as Brent alone — whole a(12) and a(13), both rules, slices of n = 14 and 15 (where the
 cycle length field of a memo entry is narrowest), a table too small to hold the cycles, and the seeded
 sample aggregates."""
 import random
@@ -24,7 +25,7 @@ def same(wl, a, b):
         assert da[k] == db[k], (k, da[k], db[k])
 
 
-@pytest.mark.parametrize("variant", [7, 15])
+@pytest.mark.parametrize("variant", [7, 15, 31])
 def test_memo_full_a12_a13(wl, golden, variant):
     for n in (12, 13):
         r = wl.enumerate_job(wl.make_job(n, hbins=256), memo_tune(wl, variant=variant))
@@ -44,7 +45,7 @@ def test_memo_rule1_a13(wl, golden):
     assert (r.done, r.cyc, r.maxfin) == (g["deals"], g["cyc"], g["longest"])
 
 
-@pytest.mark.parametrize("bits,variant", [(12, 7), (16, 7), (12, 15), (16, 14)])
+@pytest.mark.parametrize("bits,variant", [(12, 7), (16, 7), (12, 15), (16, 14), (12, 31), (16, 30)])
 def test_memo_small_table(wl, bits, variant):
     """A table far smaller than the cycles' states: most inserts are lost, lookups miss, counts stay exact."""
     job = wl.make_job(12, lo=10 ** 8, hi=2 * 10 ** 8, hbins=128)
@@ -59,6 +60,7 @@ def test_memo_slices_vs_plain(wl, n, lo, span):
         plain = wl.enumerate_plain(job)
         same(wl, wl.enumerate_job(job, memo_tune(wl)), plain)
         same(wl, wl.enumerate_job(job, memo_tune(wl, variant=15, games=1)), plain)   # all states (n <= 14)
+        same(wl, wl.enumerate_job(job, memo_tune(wl, variant=31, games=1)), plain)   # and paths
 
 
 def test_memo_random_ranges_with_sample(wl, oracle):
@@ -72,7 +74,7 @@ def test_memo_random_ranges_with_sample(wl, oracle):
                               hbins=128)
             want = oracle.enumerate_job(oracle.make_job(n, 0, job.rule, job.flags, lo, hi, 128, 0, 0, 50000, 11))
             got = wl.to_dict(wl.enumerate_job(job, memo_tune(wl, games=rnd.choice([1, 2]),
-                                                             variant=rnd.choice([6, 7, 14, 15]))))
+                                                             variant=rnd.choice([6, 7, 14, 15, 30, 31]))))
             w = oracle.to_dict(want)
             for k in FIELDS + ("hist", "endhist"):
                 assert got[k] == w[k], (n, lo, hi, k)
@@ -91,7 +93,7 @@ def test_memo_ignored_where_it_does_not_apply(wl, oracle):
 def test_memo_kept_across_jobs(wl):
     """WAR_F_MEMO_KEEP: a job that starts from the memo of the previous job of the same n and rule counts the
     same; a kept memo of another n or rule is not used (the job clears it)."""
-    t = memo_tune(wl, variant=15)
+    t = memo_tune(wl, variant=31)
     a = wl.make_job(13, lo=10 ** 9, hi=10 ** 9 + 3 * 10 ** 8, hbins=128)
     b = wl.make_job(13, flags=wl.F_MEMO_KEEP, lo=4 * 10 ** 9, hi=4 * 10 ** 9 + 3 * 10 ** 8, hbins=128)
     cold = wl.enumerate_job(b, wl.make_tune(variant=3, games=2, threads=256, defer=8))

@@ -85,7 +85,8 @@ def test_random_ranges(wl, oracle, mode):
                                   dict(variant=3, defer=4, threads=1024), dict(variant=2, window=1, defer=32, games=2),
                                   dict(variant=7, games=2, defer=8), dict(variant=6, threads=128, defer=4),
                                   dict(variant=7, window=1, memo_bits=12, defer=32), dict(variant=15, games=1, defer=16),
-                                  dict(variant=14, games=2, threads=512, memo_bits=14)])
+                                  dict(variant=14, games=2, threads=512, memo_bits=14), dict(variant=31, games=1, defer=16),
+                                  dict(variant=30, games=2, memo_bits=13, defer=4)])
 def test_tunes_agree(wl, oracle, tune):
     for job in (wl.make_job(11, rule=0, hbins=64), wl.make_job(10, wl.CANON, rule=1, flags=wl.F_DISTINCT | wl.F_SHAPE,
                                                                  hbins=256, dbins=64)):
