@@ -44,6 +44,15 @@ WORKLOADS = {
 }
 
 
+def measured_hbm_peak():
+    """(GB/s, source): the pool's measured copy bandwidth, else the stated fallback."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "MEASURED_PEAKS.json hbm_gbs (measured)"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback 6.65 TB/s"
+
+
 def space(n, mode):
     return math.factorial(n - 1) * (n - 1) if mode else math.factorial(n)
 
@@ -308,7 +317,7 @@ def main():
         barrier(ws)
         e2e_s = max_over_ranks(time.perf_counter() - t0, ws)
         h2d = 64 + 24 * 64 + 512       # job/tune structs, extra units, kernel parameter block per launch
-        d2h = 73856                      # the accumulator block read back per launch
+        d2h = 73880                      # the accumulator block read back per launch
         e2e = {"value": total / e2e_s, "unit": "positions/s" if mode else "deals/s", "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "api": "war_gpu.run" if ws == 1 else "warlib.enumerate_job"}
 
@@ -325,6 +334,16 @@ def main():
     if rank == 0:
         issue_peak, alu_peak = warlib.measure_int_peak()
         achieved = turns * K_OPS_PER_TURN / (kernel_ms * 1e-3)    # algorithmic int ops/s of the refill kernel
+        memo = None
+        if tune is not None and (tune.variant & 4) and res.memo_lookups:
+            # the cycle memo's own traffic: one 8-byte word read per lookup, one written per store
+            hbm_peak, hbm_src = measured_hbm_peak()
+            mbytes = 8.0 * (res.memo_lookups + res.memo_stores)
+            memo = {"variant": tune.variant, "table_bytes": 8 << (tune.memo_bits or 24),
+                    "lookups_per_game": res.memo_lookups / res.done, "hit_rate": res.memo_hits / res.memo_lookups,
+                    "stores_per_game": res.memo_stores / res.done, "turns_per_game": res.turns / res.done,
+                    "algorithmic_GBps": mbytes / (kernel_ms * 1e-3) / 1e9, "hbm_peak_GBps": hbm_peak,
+                    "frac_of_hbm": mbytes / (kernel_ms * 1e-3) / 1e9 / hbm_peak, "hbm_peak_source": hbm_src}
         unit = "positions/s" if mode else "deals/s"
         value = total * args.steps / (ms_max * 1e-3)
         cs = clk.summary()
@@ -346,7 +365,10 @@ def main():
                          "peak_source": "war_measure_int_peak on this GPU (LOP3+IMAD issue ceiling)"},
             "clocks": cs,
             "check": check,
+            "tune": {k: getattr(tune, k) for k, _ in tune._fields_} if tune is not None else None,
         }
+        if memo:
+            line["memo"] = memo
         if e2e:
             line["e2e"] = e2e
         if plain:

@@ -55,12 +55,24 @@ def load_cache():
     return {}
 
 
-def cached_tune(n, mode, rule, flags):
-    """The stored best war_tune for this job class on this GPU, or None."""
-    c = load_cache().get(key(n, mode, rule, flags))
-    if not c:
+def default_tune(n, mode, rule, flags):
+    """The tune for a job class with no stored entry: for deals, the path memo with a table that grows
+    with n (the n = 13 measurements: 6! work units, services every 8 turns, one game per lane); for
+    canonical scans, None (the library's defaults)."""
+    if mode != warlib.DEALS or n < 4:
         return None
-    t = c["tune"]
+    bits = {4: 12, 5: 12, 6: 14, 7: 16, 8: 18, 9: 20, 10: 22, 11: 24, 12: 27}.get(n, 30)
+    variant = 31 if n <= 14 else (7 if n == 15 else 3)
+    return {"block_m": min(6, n), "blocks_per_sm": 0, "defer": 8, "games": 1, "threads": 256, "window": 32,
+            "variant": variant, "memo_bits": bits}
+
+
+def cached_tune(n, mode, rule, flags):
+    """The stored best war_tune for this job class on this GPU, else default_tune(), or None."""
+    c = load_cache().get(key(n, mode, rule, flags))
+    t = c["tune"] if c else default_tune(n, mode, rule, flags)
+    if not t:
+        return None
     return warlib.make_tune(t["threads"], t["blocks_per_sm"], t["games"], t["block_m"], t["window"], t["defer"],
                             t.get("variant", 0), t.get("memo_bits", 0))
 
@@ -112,6 +124,8 @@ def autotune(n, mode=warlib.DEALS, rule=0, flags=0, slice_s=0.4, passes=2, verbo
     stored = load_cache().get(key(n, mode, rule, flags))
     if stored:   # start from the stored best
         cur.update(stored["tune"])
+    elif default_tune(n, mode, rule, flags):
+        cur.update(default_tune(n, mode, rule, flags))
     lo, hi = _slice(n, mode, rule, flags, slice_s, cur)
     job = warlib.make_job(n, mode, rule, flags, lo, hi, hbins=256, dbins=4096 if flags & warlib.F_DISTINCT else 0)
     best_ms, ref = measure(job, cur)

@@ -105,6 +105,7 @@ void merge_acc(const DevAcc& h, war_result* r, int hbins, int dbins) {
     r->s_count += h.s_count; r->s_cyc += h.s_cyc; r->s_lamsum += h.s_lamsum; r->s_lensum += h.s_lensum;
     if (h.s_maxfin > r->s_maxfin) r->s_maxfin = h.s_maxfin;
     r->units += h.units;
+    r->memo_lookups += h.memo_lookups; r->memo_hits += h.memo_hits; r->memo_stores += h.memo_stores;
     for (int i = 0; i < hbins; i++) r->hist[i] += h.hist[i];
     for (int i = 0; i < dbins; i++) r->dhist[i] += h.dhist[i];
     for (int i = 0; i < WAR_EBINS; i++) r->endhist[i] += h.endhist[i];

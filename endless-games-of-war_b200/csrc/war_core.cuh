@@ -193,6 +193,7 @@ __device__ __forceinline__ u64 warp_max(u64 v) {
 struct DevAcc {
     u64 cyc, done, maxfin, turns, shape_nonstd, shape_unchecked, oncycle, distinct_min;
     u64 s_count, s_cyc, s_lamsum, s_lensum, s_maxfin, units;
+    u64 memo_lookups, memo_hits, memo_stores;
     u64 work_next;   // persistent kernel: next work unit
     u64 status;      // nonzero: a game hit the turn cap
     u64 hist[WAR_HBINS_MAX];

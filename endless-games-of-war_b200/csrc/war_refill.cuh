@@ -397,8 +397,9 @@ __device__ __forceinline__ void memo_put(u64* T, u32 bits, u64 key, u32 lsh, u32
 // The path memo (MEMO_PATH) adds, for every decided game, the states at which it was looked up and
 // missed (the last two), with the game's outcome from there: "on a cycle of length lam" (value 2 lam) or
 // "ends after r more turns" (value 2r + 1).  Deals of nearby ranks often merge into one another's paths
-// after a few turns, so a later game is decided where it meets such a state.  Path entries are plain
-// stores that overwrite the slot (the most recent paths are the useful ones).
+// after a few turns, so a later game is decided where it meets such a state.  All entries of these two
+// memos are plain fire-and-forget stores that overwrite the slot (the most recent paths are the useful
+// ones; an aligned 8-byte store never tears, and a lost entry only means a later decision).
 enum { MEMO_NONE = 0, MEMO_LANDMARK = 1, MEMO_ALL = 2, MEMO_PATH = 3 };
 
 __device__ __forceinline__ u64 memo_key_state(u64 w1, u64 w2, u32 n) {
@@ -424,9 +425,8 @@ __device__ __noinline__ void memo_store_cycle(u64* T, u32 bits, u64 w1, u64 w2, 
     const u64 top = (u64)(n - 1u);
     for (u32 t = 0; t < lam; t++) {
         if (MODE == MEMO_PATH) {
-            unsigned long long* p = (unsigned long long*)T + memo_slot(memo_key_state(w1, w2, n), bits);
-            const unsigned long long val = memo_key_state(w1, w2, n) | ((u64)v << lsh);
-            if (__ldcg(p) != val) __stcg(p, val);
+            const u64 k = memo_key_state(w1, w2, n);
+            __stcg((unsigned long long*)T + memo_slot(k, bits), (unsigned long long)(k | ((u64)v << lsh)));
         } else if (MODE == MEMO_ALL) memo_put(T, bits, memo_key_state(w1, w2, n), lsh, lam);
         else if ((w1 & 15ull) == top) memo_put(T, bits, memo_key(w1, w2, n), lsh, lam);
         else if ((w2 & 15ull) == top) memo_put(T, bits, memo_key(w2, w1, n), lsh, lam);
@@ -449,8 +449,8 @@ struct LGame {
     u64 s1, s2; u32 sq; bool sampled;
     u64 m1, m2;         // MEMO_LANDMARK: the last landmark passed since the last lookup (m1 = 0: none)
     u32 mlam;           // MEMO: the memo's value for this game (0: decided by Brent or by its end)
-    u64 pa1, pa2, pb1, pb2;   // MEMO_PATH: the last two states looked up and missed,
-    u32 ta, tb;               // at these turns (0: none)
+    u64 ka, kb;         // MEMO_PATH: the keys of the last two states looked up and missed,
+    u32 ta, tb;         // at these turns (0: none)
 };
 
 // With MEMO_LANDMARK, each turn also keeps the state before it when card n-1 is on top (a landmark), and
@@ -480,6 +480,7 @@ __device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __res
     LGame<EXTRA, MEMO> g[G];
     u32 cyc = 0, done = 0, maxfin = 0, capped = 0, turns = 0;
     u32 sc = 0, scy = 0, slam = 0, slen = 0, smax = 0, oncyc = 0, dmin = 0;
+    u32 mlook = 0, mhit = 0, mstore = 0;   // memo traffic
     const u32 nm1 = n - 1u;
     u64* const memo = MEMO ? a.memo : nullptr;
     const u32 mbits = a.memo_bits, lsh = memo_lam_shift<MEMO>(n);
@@ -563,12 +564,14 @@ __device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __res
 #pragma unroll
             for (int i = 0; i < G; i++) {
                 LGame<EXTRA, MEMO>& x = g[i];
+                mlook += look[i] ? 1u : 0u;
                 if (look[i] && (e[i] & kmask) == key[i]) {   // (an empty slot reads 0, which is no key)
+                    mhit++;
                     const u32 v = (u32)(e[i] >> lsh);
                     x.done = true; x.kcy = MEMO == MEMO_PATH ? (v & 1u) == 0u : true; x.mlam = v;
                 } else if (MEMO == MEMO_PATH && look[i]) {
-                    x.pb1 = x.pa1; x.pb2 = x.pa2; x.tb = x.ta;
-                    x.pa1 = x.w1; x.pa2 = x.w2; x.ta = x.rounds;
+                    x.kb = x.ka; x.tb = x.ta;
+                    x.ka = key[i]; x.ta = x.rounds;
                 }
             }
         }
@@ -591,19 +594,21 @@ __device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __res
                         const u64 vmax = 1ull << (64u - lsh);
                         if (x.ta) {
                             const u64 v = cy ? 2ull * lam : 2ull * (len - x.ta) + 1ull;
-                            const u64 k = memo_key_state(x.pa1, x.pa2, n);
-                            if (v < vmax) __stcg((unsigned long long*)memo + memo_slot(k, mbits), k | (v << lsh));
+                            const u64 k = x.ka;
+                            if (v < vmax) { __stcg((unsigned long long*)memo + memo_slot(k, mbits), k | (v << lsh)); mstore++; }
                         }
                         if (x.tb) {
                             const u64 v = cy ? 2ull * lam : 2ull * (len - x.tb) + 1ull;
-                            const u64 k = memo_key_state(x.pb1, x.pb2, n);
-                            if (v < vmax) __stcg((unsigned long long*)memo + memo_slot(k, mbits), k | (v << lsh));
+                            const u64 k = x.kb;
+                            if (v < vmax) { __stcg((unsigned long long*)memo + memo_slot(k, mbits), k | (v << lsh)); mstore++; }
                         }
                     }
                     if (cy) {
                         cyc++;
-                        if (MEMO && memo != nullptr && mcy == 0u)   // found by Brent: store its cycle
+                        if (MEMO && memo != nullptr && mcy == 0u) {   // found by Brent: store its cycle
                             memo_store_cycle<RULE, MEMO>(memo, mbits, x.w1, x.w2, TV ? x.q + qshift : x.q, n, lam);
+                            mstore += lam;
+                        }
                         if (a.hbins) atomicAdd(&shh[lam < hb1 ? lam : hb1], 1u);
                         if (CANON && EXTRA && a.distinct) {
                             const u32 tstep = (x.next - W) >> 1;
@@ -639,6 +644,14 @@ __device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __res
         }
     }
 
+    if (MEMO) {
+        u64 v_l = warp_sum((u64)mlook), v_h = warp_sum((u64)mhit), v_s = warp_sum((u64)mstore);
+        if ((threadIdx.x & 31) == 0) {
+            if (v_l) atomicAdd(&acc->memo_lookups, v_l);
+            if (v_h) atomicAdd(&acc->memo_hits, v_h);
+            if (v_s) atomicAdd(&acc->memo_stores, v_s);
+        }
+    }
     u64 v_cyc = warp_sum(cyc), v_done = warp_sum(done), v_turns = warp_sum((u64)turns), v_max = warp_max(maxfin);
     u64 v_cap = warp_sum(capped);
     if ((threadIdx.x & 31) == 0) {

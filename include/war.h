@@ -110,6 +110,7 @@ typedef struct war_result {
     uint64_t distinct_min;   /* positions that are the minimum canonical state of their cycle (= distinct cycles) */
     uint64_t s_count, s_cyc, s_lamsum, s_lensum, s_maxfin; /* sample aggregates (WAR_F_SAMPLE) */
     uint64_t units;          /* work units processed (diagnostic) */
+    uint64_t memo_lookups, memo_hits, memo_stores; /* cycle memo traffic (war_tune.variant bit 2; diagnostic) */
     double kernel_ms;        /* device time of the enumeration kernel(s), CUDA events */
     int32_t hbins, dbins, blk, status;
     uint64_t hist[WAR_HBINS_MAX];
