@@ -32,6 +32,9 @@ sys.path.insert(0, PKG)
 # under the winner: 22), Brent's test and bookkeeping (6), the end test (2).  Fixed from the source of
 # war_turn / batched_kernel, not from compiled code.
 K_OPS_PER_TURN = 30
+# DRAM bytes (read + write) per deal of the path-memo refill kernel, from an ncu capture of the second span
+# of `war_gpu.py 13 --hist 256` (1.94e9 deals, 214.6 GB): the random memo reads cost ~108 B each.
+MEMO_DRAM_BYTES_PER_DEAL = 110.8
 
 WORKLOADS = {
     "deals13": dict(n=13, mode=0, hbins=256, flags=0, label="n=13 all deals (war_gpu.py 13 --hist 256)"),
@@ -361,7 +364,10 @@ def main():
             "roofline": {"bound": "int_issue", "achieved": achieved / 1e12, "peak": issue_peak / 1e12,
                          "unit": "Tops/s (INT32 thread-ops)", "frac": achieved / issue_peak,
                          "alu_pipe_peak": alu_peak / 1e12, "frac_of_alu_pipe": achieved / alu_peak,
-                         "ops_per_turn": K_OPS_PER_TURN, "traffic": None,
+                         "ops_per_turn": K_OPS_PER_TURN,
+                         "traffic": (MEMO_DRAM_BYTES_PER_DEAL * total / max(1, launches // args.steps)
+                                     if memo and mode == 0 and n == 13 else None),
+                         "traffic_unit": "DRAM bytes per launch (ncu capture scaled by deals per launch)",
                          "peak_source": "war_measure_int_peak on this GPU (LOP3+IMAD issue ceiling)"},
             "clocks": cs,
             "check": check,

@@ -27,8 +27,9 @@ sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
 import warlib  # noqa: E402
 
 # Ranks enumerated per call of the engine: a few seconds of work, so progress is written about as
-# often as the reference writes it (every 10 s) and an interrupted run loses little.
-SPAN_RANKS = 1 << 32
+# often as the reference writes it (every 10 s) and an interrupted run loses little.  Just under 2^32,
+# so that a span of deals is one launch of the engine (a launch plays fewer than 2^32 - 2^24 games).
+SPAN_RANKS = (1 << 32) - (1 << 25)
 
 
 def _tune_for(n, canon, rule, flags):
@@ -37,6 +38,19 @@ def _tune_for(n, canon, rule, flags):
         return autotune.cached_tune(n, warlib.CANON if canon else warlib.DEALS, rule, flags)
     except Exception:
         return None
+
+
+def override_tune(tune, fields):
+    """A copy of tune (a warlib.Tune or None) with the given fields replaced."""
+    t = warlib.make_tune()
+    if tune is not None:
+        for k, _ in warlib.Tune._fields_:
+            setattr(t, k, getattr(tune, k))
+    for k, v in fields.items():
+        if k not in dict(warlib.Tune._fields_):
+            raise ValueError("unknown tune field %r" % k)
+        setattr(t, k, int(v))
+    return t
 
 
 def run(n, half=False, per=256, threads=256, batch_threads=1 << 18, out=None, resume=False, quiet=False, hbins=0,
@@ -171,15 +185,22 @@ def main(argv=None):
                     help="canon only: check every loop alternates in runs of exactly 2^v (Spivey Thm 3 type)")
     ap.add_argument("--plain", action="store_true",
                     help="use the plain kernel (the reference's per-thread blocks) instead of the refill kernel")
+    ap.add_argument("--tune", default=None,
+                    help='JSON object overriding fields of the stored tune, e.g. \'{"memo_bits": 28}\'')
     a = ap.parse_args(argv)
     if a.hist > warlib.WAR_HBINS_MAX:
         ap.error("--hist is at most %d" % warlib.WAR_HBINS_MAX)
     lo = a.nmin if a.nmin is not None else a.nmax
     for n in range(lo, a.nmax + 1):
         half = a.half and n % 2 == 0 and not a.canon
+        tune = None
+        if a.tune and not a.plain:
+            flags = (warlib.F_HALF if half else 0) | (warlib.F_DISTINCT if a.distinct else 0) | \
+                (warlib.F_SHAPE if a.shape and a.canon else 0)
+            tune = override_tune(_tune_for(n, a.canon, a.rule, flags), json.loads(a.tune))
         c, d, mx, el, h, sh, dd = run(n, half=half, per=a.per, out=a.out, resume=a.resume,
                                       quiet=a.out is None, hbins=a.hist, canon=a.canon, shape=a.shape,
-                                      rule=a.rule, dbins=4096 if a.distinct else 0, plain=a.plain)
+                                      rule=a.rule, dbins=4096 if a.distinct else 0, plain=a.plain, tune=tune)
         expect = math.factorial(n - 1) * (n - 1) if a.canon else math.factorial(n)
         assert d == expect, (d, expect)
         if h:
