@@ -18,7 +18,7 @@ typedef void (*BatchedFn)(const BatchArgs, DevAcc*);
 template <int RULE, int G, int V>
 static BatchedFn pick_g(int canon, int shape, int extra) {
     if (!canon) return extra ? batched_kernel<RULE, G, false, false, true, V> : batched_kernel<RULE, G, false, false, false, V>;
-    if constexpr ((V & 4) != 0) return nullptr;   // the cycle memo serves deals only
+    if constexpr ((V & 4) != 0 && (V & 16) == 0) return nullptr;   // canonical scans: the path memo only
     if (shape) return extra ? batched_kernel<RULE, G, true, true, true, V> : batched_kernel<RULE, G, true, true, false, V>;
     return extra ? batched_kernel<RULE, G, true, false, true, V> : batched_kernel<RULE, G, true, false, false, V>;
 }
@@ -32,7 +32,7 @@ static BatchedFn pick_v(int canon, int rule, int shape, int extra, int games) {
 // variant: bit 0 = multiply-add turn form, bit 1 = latched records, bit 2 = cycle memo (deals, latched),
 // bit 3 = the memo holds every cycle state (else landmarks), bit 4 = and the paths of decided games
 static BatchedFn pick(int canon, int rule, int shape, int extra, int games, int variant) {
-    if (canon || (variant & 2) == 0) variant &= 3;
+    if ((variant & 2) == 0 || (canon && (variant & 16) == 0)) variant &= 3;
     if ((variant & 4) == 0) variant &= 7;
     if ((variant & 8) == 0) variant &= 15;
     switch (variant) {

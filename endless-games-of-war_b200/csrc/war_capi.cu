@@ -210,8 +210,10 @@ int resolve_tune(const war_job* job, const war_tune* in, Tune& t) {
     if (t.defer < 1 || t.defer > 32) return fail(WAR_EINVAL, "tune.defer=%d (1..32)", t.defer);
     if (t.variant < 0 || t.variant > 31) return fail(WAR_EINVAL, "tune.variant=%d (0..31)", t.variant);
     if (t.memo_bits < 12 || t.memo_bits > 31) return fail(WAR_EINVAL, "tune.memo_bits=%d (12..31)", t.memo_bits);
-    // the cycle memo serves deals of 4..15 cards with latched records; all states up to 14 cards
-    if ((t.variant & 4) && (canon || !(t.variant & 2) || job->n < 4 || job->n > 15)) t.variant &= 3;
+    // the cycle memo serves deals of 4..15 cards with latched records, all states up to 14 cards;
+    // canonical scans take the path memo only
+    if ((t.variant & 4) && (!(t.variant & 2) || job->n < 4 || job->n > 15)) t.variant &= 3;
+    if (canon && !(t.variant & 16)) t.variant &= 3;
     if ((t.variant & 8) && job->n > 14) t.variant &= 7;
     if (!(t.variant & 4)) t.variant &= 7;
     if (!(t.variant & 8)) t.variant &= 15;

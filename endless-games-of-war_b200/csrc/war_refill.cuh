@@ -451,6 +451,7 @@ struct LGame {
     u32 mlam;           // MEMO: the memo's value for this game (0: decided by Brent or by its end)
     u64 ka, kb;         // MEMO_PATH: the keys of the last two states looked up and missed,
     u32 ta, tb;         // at these turns (0: none)
+    u32 pend;           // canonical distinct scan: the memo's cycle length, held until turn pend (0: none)
 };
 
 // With MEMO_LANDMARK, each turn also keeps the state before it when card n-1 is on top (a landmark), and
@@ -494,6 +495,7 @@ __device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __res
         x.done = !ok; x.kcy = false;
         if (MEMO) { x.m1 = 0ull; x.m2 = 0ull; x.mlam = 0u; }
         if (MEMO == MEMO_PATH) { x.ta = 0u; x.tb = 0u; }
+        if (MEMO) x.pend = 0u;
         if (EXTRA) {
             x.s1 = x.w1; x.s2 = x.w2; x.sq = x.q;
             x.sampled = a.sample && ok && war_pick(a.seed, a.thr, x.w1, x.w2);
@@ -551,7 +553,7 @@ __device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __res
             for (int i = 0; i < G; i++) {
                 LGame<EXTRA, MEMO>& x = g[i];
                 if (MEMO >= MEMO_ALL) {
-                    look[i] = !x.done;
+                    look[i] = !x.done & (x.pend == 0u);
                     key[i] = memo_key_state(x.w1, x.w2, n);
                 } else {
                     look[i] = !x.done & (x.m1 != 0ull);
@@ -568,7 +570,19 @@ __device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __res
                 if (look[i] && (e[i] & kmask) == key[i]) {   // (an empty slot reads 0, which is no key)
                     mhit++;
                     const u32 v = (u32)(e[i] >> lsh);
-                    x.done = true; x.kcy = MEMO == MEMO_PATH ? (v & 1u) == 0u : true; x.mlam = v;
+                    const bool vcy = MEMO == MEMO_PATH ? (v & 1u) == 0u : true;
+                    const u32 vlam = MEMO == MEMO_PATH ? v >> 1 : v;
+                    if (CANON && EXTRA && a.distinct && vcy && vlam <= W && x.rounds < vlam) {
+                        // Whether the start lies on its cycle shows at turn vlam: Brent's first window
+                        // compares every state up to W >= vlam with the start.  Play on until then.
+                        x.pend = vlam;
+                    } else {
+                        x.done = true; x.kcy = vcy; x.mlam = v;
+                    }
+                } else if (CANON && EXTRA && x.pend != 0u && !x.done && x.rounds >= x.pend) {
+                    // turn pend passed without the start coming back: on the cycle of length pend, not
+                    // through the start
+                    x.done = true; x.kcy = true; x.mlam = MEMO == MEMO_PATH ? 2u * x.pend : x.pend;
                 } else if (MEMO == MEMO_PATH && look[i]) {
                     x.kb = x.ka; x.tb = x.ta;
                     x.ka = key[i]; x.ta = x.rounds;
@@ -612,7 +626,10 @@ __device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __res
                         if (a.hbins) atomicAdd(&shh[lam < hb1 ? lam : hb1], 1u);
                         if (CANON && EXTRA && a.distinct) {
                             const u32 tstep = (x.next - W) >> 1;
-                            bool on = (tstep == 0u) ? true
+                            // decided by the memo: the start was not seen again within lam <= W turns
+                            // (else Brent's first window would have decided it), or lam > W: walk
+                            bool on = (MEMO && mcy) ? (lam <= W ? false : on_cycle_walk<RULE>(x.s1, x.s2, x.sq, n, lam))
+                                    : (tstep == 0u) ? true
                                     : (lam <= W ? false : on_cycle_walk<RULE>(x.s1, x.s2, x.sq, n, lam));
                             if (on) {
                                 CycleWalk cw = cycle_walk<RULE>(x.s1, x.s2, x.sq, n, lam);
@@ -685,7 +702,7 @@ template <int RULE, int G, bool CANON, bool SHAPE, bool EXTRA, int V>
 __device__ __forceinline__ void refill_dispatch(const BatchArgs& a, DevAcc* __restrict__ acc, u64* __restrict__ counter,
                                                 u32* sh) {
     if constexpr (SHAPE || (V & 2) == 0) refill_body<RULE, G, CANON, SHAPE, EXTRA, V & 1>(a, acc, counter, sh);
-    else if constexpr (CANON || (V & 4) == 0) refill_latched<RULE, G, CANON, EXTRA, V & 1, MEMO_NONE>(a, acc, counter, sh);
+    else if constexpr ((V & 4) == 0 || (CANON && (V & 8) == 0)) refill_latched<RULE, G, CANON, EXTRA, V & 1, MEMO_NONE>(a, acc, counter, sh);
     else if constexpr ((V & 24) == 24) refill_latched<RULE, G, CANON, EXTRA, V & 1, MEMO_PATH>(a, acc, counter, sh);
     else if constexpr ((V & 8) != 0) refill_latched<RULE, G, CANON, EXTRA, V & 1, MEMO_ALL>(a, acc, counter, sh);
     else refill_latched<RULE, G, CANON, EXTRA, V & 1, MEMO_LANDMARK>(a, acc, counter, sh);

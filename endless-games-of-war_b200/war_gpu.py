@@ -104,7 +104,7 @@ def run(n, half=False, per=256, threads=256, batch_threads=1 << 18, out=None, re
         tl = time.time()
         end = min(total, start + span)
         # spans after the first keep the cycle memo of the one before (same n and rule)
-        keep = warlib.F_MEMO_KEEP if (start > first and not canon) else 0
+        keep = warlib.F_MEMO_KEEP if start > first else 0
         job = warlib.make_job(n, mode, rule, flags | keep, start * mult_pos, end * mult_pos, hbins=hbins, dbins=dbins,
                               blk=blk)
         r = warlib.enumerate_plain(job) if plain else warlib.enumerate_job(job, tune)

@@ -50,7 +50,7 @@ enum war_flags {
     WAR_F_DISTINCT = 2, /* canon: distinct-cycle weights + min-key count (gpu/war_gpu.py:217-235, cpu/distinct_cycles.c:67-80) */
     WAR_F_SHAPE = 4,    /* canon: Theorem-3 loop-shape test, blk = n & -n (gpu/war_gpu.py:51-73, :290) */
     WAR_F_SAMPLE = 8,   /* accumulate the seeded sample aggregates used by the Floyd cross-check */
-    WAR_F_MEMO_KEEP = 16 /* deals with the cycle memo (war_tune.variant bit 2): start from the memo left by the
+    WAR_F_MEMO_KEEP = 16 /* jobs with the cycle memo (war_tune.variant bit 2): start from the memo left by the
                             previous war_enumerate of the same n and rule instead of an empty one (its entries
                             are facts about n and the rule, not about the range); no other effect (no
                             reference counterpart) */
@@ -84,8 +84,8 @@ typedef struct war_tune {
     int32_t defer;         /* immediate records: lanes that wait, decided, before the warp refills them (1..32);
                               latched records: iterations between services (rounded up to a multiple of 4) */
     int32_t variant;       /* bit 0: multiply-add turn form (else logic/shift); bit 1: outcomes latched and
-                              recorded every `defer` iterations (else recorded at once); bit 2 (deals with
-                              bit 1, n <= 15): cycle memo, a game is decided as soon as it passes a state of
+                              recorded every `defer` iterations (else recorded at once); bit 2 (with
+                              bit 1, n <= 15; canonical scans only with bits 3 and 4): cycle memo, a game is decided as soon as it passes a state of
                               a cycle found before in the job (`turns` then counts the turns played, fewer
                               than the reference's schedule); bit 3 (with bit 2, n <= 14): the memo holds
                               every state of the found cycles and games are looked up at their current

@@ -105,3 +105,47 @@ def test_memo_kept_across_jobs(wl):
     same(wl, wl.enumerate_job(b, t), cold)   # the rule-1 n = 12 memo is not kept for n = 13 rule 0
     c = wl.make_job(12, flags=wl.F_MEMO_KEEP, lo=2 * 10 ** 8, hi=4 * 10 ** 8, hbins=128)
     same(wl, wl.enumerate_job(c, t), wl.enumerate_plain(wl.make_job(12, lo=2 * 10 ** 8, hi=4 * 10 ** 8, hbins=128)))
+
+
+@pytest.mark.parametrize("variant", [30, 31])
+def test_memo_canon_small_vs_oracle(wl, oracle, variant):
+    """Canonical scans with the path memo: cycling count, λ-histogram, ending lengths, the distinct-cycle
+    outputs (on-cycle starts, min keys, weights) and the sample aggregates equal the oracle's."""
+    for n in (5, 7, 9, 10, 11):
+        for rule in (0, 1):
+            job = wl.make_job(n, wl.CANON, rule=rule, flags=wl.F_DISTINCT | wl.F_SAMPLE, hbins=256, dbins=256,
+                              sample_ppm=30000, seed=5)
+            want = oracle.to_dict(oracle.enumerate_job(oracle.make_job(n, 1, rule, job.flags, 0, job.hi, 256, 256, 0,
+                                                                       30000, 5)))
+            got = wl.to_dict(wl.enumerate_job(job, memo_tune(wl, variant=variant, window=128, memo_bits=20)))
+            for k in FIELDS + ("hist", "dhist", "endhist"):
+                assert got[k] == want[k], (n, rule, k)
+
+
+def test_memo_canon_random_ranges(wl, oracle):
+    rnd = random.Random(77)
+    for n in (9, 10, 11):
+        total = wl.space_size(n, wl.CANON)
+        for _ in range(3):
+            lo = rnd.randrange(0, total)
+            hi = min(total, lo + rnd.choice([1, 50, 7777, 300000]))
+            job = wl.make_job(n, wl.CANON, rule=rnd.randint(0, 1), flags=wl.F_DISTINCT, lo=lo, hi=hi, hbins=128,
+                              dbins=128)
+            want = oracle.to_dict(oracle.enumerate_job(oracle.make_job(n, 1, job.rule, job.flags, lo, hi, 128, 128)))
+            got = wl.to_dict(wl.enumerate_job(job, memo_tune(wl, variant=31, window=128)))
+            for k in FIELDS + ("hist", "dhist", "endhist"):
+                assert got[k] == want[k], (n, lo, hi, k)
+
+
+def test_memo_canon_n13_n14_full(wl, golden):
+    """The n = 13 and n = 14 canonical scans with --distinct and the path memo: the recorded cycling,
+    on-cycle and distinct counts and the weights."""
+    for n in (13, 14):
+        job = wl.make_job(n, wl.CANON, flags=wl.F_DISTINCT, hbins=256, dbins=4096)
+        r = wl.to_dict(wl.enumerate_job(job, memo_tune(wl, window=128, memo_bits=28)))
+        g = golden["canon_table"][n]
+        assert (r["cyc"], r["oncycle"], r["done"]) == (g["cycling"], g["oncycle"], g["positions"])
+        assert sum(v // k for k, v in r["dhist"].items()) == g["distinct"]
+        plain = wl.to_dict(wl.enumerate_job(job))   # the same scan without the memo
+        for k in FIELDS + ("hist", "dhist", "endhist"):
+            assert r[k] == plain[k], (n, k)
