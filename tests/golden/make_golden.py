@@ -112,6 +112,16 @@ def main():
                                  "hist": parse_hist(m.group(6)) if m.group(6) else {}}
     g["war_gpu_deals_hist"] = hists
 
+    # the printed lines themselves (the drop-in CLI must print them byte for byte apart from the time):
+    # deals n = 1..13 with --hist 256, canonical n = 1..13 with --distinct --shape (checks.txt:5-24, 143-182)
+    def out_lines(text):
+        return [ln for ln in text.split("\n") if ln.startswith("n=") or ln.startswith("   ")]
+    g["war_gpu_lines"] = {
+        "deals_hist256": out_lines(checks.split("== Deals, n = 1..13")[1].split("==")[0]),
+        "canon_distinct_shape": out_lines(
+            checks.split("== Canonical positions, distinct cycles and the Theorem-3 test, n = 1..13")[1].split("==")[0]),
+    }
+
     # n = 14, 15 long deal runs with histograms (long_runs.txt:13-17)
     lr = {}
     for m in re.finditer(r"n=(\d+)  a\(n\)=(\d+)  of (\d+)  longest finite=(\d+) rounds  [\d.]+s(  \(half\))?\n"

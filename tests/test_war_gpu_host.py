@@ -1,0 +1,98 @@
+"""The drop-in runner's host logic on the CPU (gpu/war_gpu.py:272-398): with the oracle standing in for
+the engine, `war_gpu.main` prints the reference's recorded output lines byte for byte apart from the time,
+an interrupted run resumes from its progress file to the same result, and every span of a run after its
+first asks the engine to keep the cycle memo."""
+import io
+import json
+import re
+import contextlib
+
+import pytest
+
+TIME = re.compile(r"  [0-9.]+s")
+
+
+def fake_engine(monkeypatch, oracle, calls=None, fail_after=None):
+    """Replaces the engine entry points with the oracle on the same job (the oracle is the checker here:
+    what is under test is the host code around the engine)."""
+    import warlib
+    import war_gpu
+
+    def enum(job, tune=None):
+        if calls is not None:
+            calls.append((job.lo, job.hi, job.flags))
+            if fail_after is not None and len(calls) > fail_after:
+                raise KeyboardInterrupt("interrupted by the test")
+        return oracle.enumerate_job(oracle.make_job(job.n, job.mode, job.rule, job.flags & ~warlib.F_MEMO_KEEP,
+                                                    job.lo, job.hi, job.hbins, job.dbins, job.blk, job.sample_ppm,
+                                                    job.seed))
+    monkeypatch.setattr(warlib, "enumerate_job", enum)
+    monkeypatch.setattr(warlib, "enumerate_plain", enum)
+    monkeypatch.setattr(war_gpu, "_tune_for", lambda *a: None)
+
+
+def main_lines(argv):
+    import war_gpu
+    buf = io.StringIO()
+    with contextlib.redirect_stdout(buf):
+        war_gpu.main(argv)
+    return [TIME.sub("  Xs", ln) for ln in buf.getvalue().splitlines()]
+
+
+def recorded(golden, name, nmax):
+    out, keep = [], False
+    for ln in golden["war_gpu_lines"][name]:
+        if ln.startswith("n="):
+            keep = int(ln.split()[0][2:]) <= nmax
+        if keep:
+            out.append(TIME.sub("  Xs", ln))
+    return out
+
+
+def test_deal_lines_match_the_recorded_output(monkeypatch, oracle, golden):
+    """`war_gpu.py 11 --nmin 1 --hist 256` (data/checks.txt:5-24, n <= 11)."""
+    fake_engine(monkeypatch, oracle)
+    assert main_lines(["11", "--nmin", "1", "--hist", "256"]) == recorded(golden, "deals_hist256", 11)
+
+
+def test_canonical_lines_match_the_recorded_output(monkeypatch, oracle, golden):
+    """`war_gpu.py 10 --nmin 1 --canon --distinct --shape` (data/checks.txt:143-182, n <= 10)."""
+    fake_engine(monkeypatch, oracle)
+    assert main_lines(["10", "--nmin", "1", "--canon", "--distinct", "--shape"]) == \
+        recorded(golden, "canon_distinct_shape", 10)
+
+
+def test_interrupted_run_resumes_to_the_same_result(monkeypatch, oracle, tmp_path):
+    import war_gpu
+    monkeypatch.setattr(war_gpu, "SPAN_RANKS", 40000)
+    full = None
+    fake_engine(monkeypatch, oracle)
+    kw = dict(hbins=64, per=16, batch_threads=256)      # spans of SPAN_RANKS deals
+    full = war_gpu.run(9, quiet=True, **kw)
+
+    calls = []
+    fake_engine(monkeypatch, oracle, calls=calls, fail_after=3)
+    out = str(tmp_path / "run9")
+    with pytest.raises(KeyboardInterrupt):
+        war_gpu.run(9, out=out, quiet=True, **kw)
+    with open(out + ".progress") as f:
+        st = json.load(f)
+    assert st["n"] == 9 and 0 < st["next_start"] < 362880
+    assert calls[0][2] & 16 == 0 and all(c[2] & 16 for c in calls[1:])   # WAR_F_MEMO_KEEP after the first span
+
+    calls2 = []
+    fake_engine(monkeypatch, oracle, calls=calls2)
+    again = war_gpu.run(9, out=out, resume=True, quiet=True, **kw)
+    assert calls2[0][0] == st["next_start"] and calls2[0][2] & 16 == 0   # a new process starts a new memo
+    assert again[:3] == full[:3] and again[4] == full[4]
+    with open(out + ".progress") as f:
+        assert json.load(f)["next_start"] == 362880
+
+
+def test_tune_override_fields(monkeypatch):
+    import warlib
+    import war_gpu
+    t = war_gpu.override_tune(warlib.make_tune(threads=256, variant=31, memo_bits=30), {"memo_bits": 28})
+    assert (t.threads, t.variant, t.memo_bits) == (256, 31, 28)
+    with pytest.raises(ValueError):
+        war_gpu.override_tune(None, {"no_such_field": 1})
