@@ -11,8 +11,13 @@
 // different n and mode therefore run side by side on the device.  Two ticks are in flight at a time (the
 // next one is queued before the previous one is waited for), so the GPU does not wait for the host; a job
 // whose last task was in a finished tick is read back, its slot freed and its result published.
+//
+// Jobs of the same n and rule share one cycle memo (war_refill.cuh): its entries are facts about n and the
+// rule, so every job of that class, now and later, decides its games from what the earlier ones found.
+// The tables are allocated when the first job of a class is admitted and kept until the server ends.
 #include <cuda_runtime.h>
 #include <algorithm>
+#include <cmath>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -54,19 +59,23 @@ static ServeFn serve_pick(bool canon, bool shape, bool extra) {
     return extra ? serve_kernel<RULE, G, true, false, true, V> : serve_kernel<RULE, G, true, false, false, V>;
 }
 
-// Launch shapes of the serving kernel: deals 2 games per thread, 128-thread blocks; canonical positions
-// 1 game per thread, 256-thread blocks; both the multiply-add turn form.
+// Launch shapes of the serving kernel: one game per thread, 256-thread blocks, the multiply-add turn form;
+// latched records with the path memo where it applies (memo = 1: n <= 14 and a table), latched records
+// without it otherwise, and the immediate-record loop for the loop-shape test.
 struct Variant {
-    int canon, rule, shape, extra;
+    int canon, rule, shape, extra, memo;
     bool operator<(const Variant& o) const {
-        return std::tie(canon, rule, shape, extra) < std::tie(o.canon, o.rule, o.shape, o.extra);
+        return std::tie(canon, rule, shape, extra, memo) < std::tie(o.canon, o.rule, o.shape, o.extra, o.memo);
     }
     bool operator==(const Variant& o) const { return !(*this < o) && !(o < *this); }
-    int games() const { return canon ? 1 : 2; }
-    int threads() const { return canon ? 256 : 128; }
+    int games() const { return 1; }
+    int threads() const { return 256; }
     ServeFn fn() const {
-        if (rule) return canon ? serve_pick<1, 1, 1>(true, shape, extra) : serve_pick<1, 2, 1>(false, false, extra);
-        return canon ? serve_pick<0, 1, 1>(true, shape, extra) : serve_pick<0, 2, 1>(false, false, extra);
+        const bool c = canon != 0;
+        if (rule) return shape ? serve_pick<1, 1, 1>(c, true, extra)
+                             : memo ? serve_pick<1, 1, 31>(c, false, extra) : serve_pick<1, 1, 3>(c, false, extra);
+        return shape ? serve_pick<0, 1, 1>(c, true, extra)
+                     : memo ? serve_pick<0, 1, 31>(c, false, extra) : serve_pick<0, 1, 3>(c, false, extra);
     }
 };
 
@@ -110,6 +119,7 @@ struct war_server {
     std::deque<uint64_t> pending;
     std::map<uint64_t, war::SJob> jobs;
     std::vector<int> free_slots;
+    std::map<std::pair<int, int>, std::pair<u64*, int>> memos;   // (n, rule) -> (table, log2 words)
     DevAcc* d_slots = nullptr;
     DevAcc* h_slot = nullptr;   // pinned readback buffer
     cudaStream_t s_comp = nullptr, s_copy = nullptr;
@@ -141,7 +151,7 @@ void set_args(war_server* s, SJob& J) {
     a.dbins = job.dbins;
     a.blk = (job.flags & WAR_F_SHAPE) && canon ? (job.blk ? job.blk : (job.n & -job.n)) : 0;
     a.W = canon ? 128 : 32;
-    a.defer = 8;
+    a.defer = canon ? 16 : 8;
     a.tk.k16 = 16u; a.tk.km16 = (u32)-16; a.tk.k2p28 = 1u << 28; a.tk.k4 = 4u; a.tk.one = 1u;
     a.tk.c0 = 2 * job.n - 4; a.tk.end2 = (u32)(4 * job.n * job.n);
     a.half = (job.flags & WAR_F_HALF) ? 1 : 0;
@@ -153,7 +163,29 @@ void set_args(war_server* s, SJob& J) {
     J.var.rule = job.rule;
     J.var.shape = a.blk ? 1 : 0;
     J.var.extra = (a.distinct || a.sample) ? 1 : 0;
-    (void)s;
+    J.var.memo = 0;
+    if (!a.blk && job.n >= 4 && job.n <= 14 && s->cfg.memo_bits >= 0) {
+        // the class's table: 2^bits words, grown with n (about a thousandth of the class's rank space)
+        const std::pair<int, int> cls(job.n, job.rule);
+        auto it = s->memos.find(cls);
+        if (it == s->memos.end()) {
+            const int cap = s->cfg.memo_bits ? s->cfg.memo_bits : 28;
+            const int bits = std::max(12, std::min(cap, 4 + (int)std::ceil(std::log2((double)fact(job.n)) * 0.75)));
+            u64* t = nullptr;
+            if (cudaMalloc(&t, sizeof(u64) << bits) != cudaSuccess ||
+                cudaMemsetAsync(t, 0, sizeof(u64) << bits, s->s_comp) != cudaSuccess) {
+                if (t) cudaFree(t);
+                t = nullptr;
+                cudaGetLastError();   // no table: the class runs without the memo
+            }
+            it = s->memos.emplace(cls, std::make_pair(t, bits)).first;
+        }
+        if (it->second.first) {
+            a.memo = it->second.first;
+            a.memo_bits = (u32)it->second.second;
+            J.var.memo = 1;
+        }
+    }
 }
 
 bool remaining(const SJob& J) { return J.next_main < J.plan.main_count || (!J.extras_issued && !J.plan.extra.empty()); }
@@ -199,7 +231,7 @@ void admit(war_server* s, Tick& T) {
             continue;
         }
         const int M = canon ? job.n - 1 : job.n;
-        make_plan(&job, std::max(1, std::min(canon ? 4 : 5, M)), J.plan);
+        make_plan(&job, std::max(1, std::min(canon ? 4 : 6, M)), J.plan);
         J.per_unit = fact(J.plan.m) * J.plan.games_per_order;
         set_args(s, J);
         J.slot = s->free_slots.back();
@@ -500,6 +532,8 @@ int war_server_destroy(war_server* s) {
         if (T.d_units) cudaFree(T.d_units);
         if (T.ev) cudaEventDestroy(T.ev);
     }
+    for (auto& kv : s->memos)
+        if (kv.second.first) cudaFree(kv.second.first);
     if (s->d_slots) cudaFree(s->d_slots);
     if (s->h_slot) cudaFreeHost(s->h_slot);
     if (s->s_comp) cudaStreamDestroy(s->s_comp);

@@ -27,9 +27,9 @@ SIZEOF_DEVACC = 19 * 8 + (warlib.WAR_HBINS_MAX + warlib.WAR_DBINS_MAX + warlib.W
 
 
 class Server:
-    def __init__(self, max_jobs=256, queue_cap=1 << 16, mem_budget=0, tick_ranks=0):
+    def __init__(self, max_jobs=256, queue_cap=1 << 16, mem_budget=0, tick_ranks=0, memo_bits=0):
         self.h = ctypes.c_void_p()
-        cfg = warlib.ServerCfg(max_jobs, queue_cap, mem_budget, tick_ranks, 0, 0)
+        cfg = warlib.ServerCfg(max_jobs, queue_cap, mem_budget, tick_ranks, 0, 0, memo_bits)
         warlib.check(warlib.lib().war_server_create(ctypes.byref(cfg), ctypes.byref(self.h)), "war_server_create")
 
     def submit(self, job):

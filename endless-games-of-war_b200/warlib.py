@@ -58,7 +58,7 @@ class Result(ctypes.Structure):
 class ServerCfg(ctypes.Structure):
     _fields_ = [("max_jobs", ctypes.c_int32), ("queue_cap", ctypes.c_int32), ("mem_budget", ctypes.c_uint64),
                 ("tick_ranks", ctypes.c_uint64), ("threads", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32),
-                ("reserved", ctypes.c_int32 * 4)]
+                ("memo_bits", ctypes.c_int32), ("reserved", ctypes.c_int32 * 3)]
 
 
 class JobStatus(ctypes.Structure):
@@ -88,6 +88,8 @@ SYMBOLS = {
     "war_enumerate": (ctypes.c_int, [ctypes.POINTER(Job), ctypes.POINTER(Tune), ctypes.POINTER(Result)]),
     "war_floyd_sample": (ctypes.c_int, [ctypes.POINTER(Job), ctypes.POINTER(Result)]),
     "war_enumerate_noalloc": (ctypes.c_int, [ctypes.POINTER(Job), ctypes.POINTER(Tune), ctypes.POINTER(Result)]),
+    "war_autotune": (ctypes.c_int, [ctypes.POINTER(Job), ctypes.POINTER(Tune), ctypes.c_double, ctypes.c_int32,
+                                    ctypes.POINTER(Tune), ctypes.POINTER(ctypes.c_double)]),
     "war_server_create": (ctypes.c_int, [ctypes.POINTER(ServerCfg), ctypes.POINTER(ctypes.c_void_p)]),
     "war_server_submit": (ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(Job), U64P]),
     "war_server_poll": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(Result), ctypes.POINTER(JobStatus)]),
@@ -156,6 +158,14 @@ def enumerate_job(job, tune=None):
     check(lib().war_enumerate(ctypes.byref(job), ctypes.byref(tune) if tune is not None else None, ctypes.byref(r)),
           "war_enumerate")
     return r
+
+
+def autotune_native(job, start=None, slice_ms=400.0, passes=2):
+    """war_autotune: (best war_tune, its kernel ms) for the job's class, searched in the library."""
+    best, ms = Tune(), ctypes.c_double()
+    check(lib().war_autotune(ctypes.byref(job), ctypes.byref(start) if start is not None else None, slice_ms, passes,
+                             ctypes.byref(best), ctypes.byref(ms)), "war_autotune")
+    return best, ms.value
 
 
 def enumerate_noalloc(job, tune=None):

@@ -176,7 +176,9 @@ typedef struct war_server_cfg {
     uint64_t mem_budget;     /* bytes of device memory the server may hold for job accumulators; 0 = free memory / 2 */
     uint64_t tick_ranks;     /* ranks issued per tick across all jobs (0 = default) */
     int32_t threads, blocks_per_sm;
-    int32_t reserved[4];
+    int32_t memo_bits;       /* cycle memo shared by all jobs of one n and rule, log2 of its 8-byte words
+                                (grown with n up to this; 0 = 28, i.e. 2 GiB per class; < 0 = no memo) */
+    int32_t reserved[3];
 } war_server_cfg;
 
 typedef struct war_job_status {
@@ -184,6 +186,15 @@ typedef struct war_job_status {
     int32_t status;          /* war_status of a failed job */
     double submit_ms, admit_ms, finish_ms; /* host clock (ms since the server started) */
 } war_job_status;
+
+/* Coordinate descent over war_tune for the class of `job` (block_m, games, threads, blocks per SM, window,
+ * defer, variant, memo_bits), timed by war_enumerate's kernel time on a slice of job's range from its
+ * middle, sized to take about slice_ms (0 = 400 ms); starts from *start (NULL = the library defaults) and
+ * makes at most `passes` passes (1..8).  Every configuration tried must return the first one's counts,
+ * else WAR_EINVAL.  The memo variants only pay on long slices (a memo is cleared per job).  The search of
+ * endless-games-of-war_b200/autotune.py, callable without Python; no counterpart in the reference. */
+int war_autotune(const war_job* job, const war_tune* start, double slice_ms, int32_t passes, war_tune* best,
+                 double* best_ms);
 
 int war_server_create(const war_server_cfg* cfg, war_server** out);
 /* Queue a job; *id receives its id.  Returns WAR_EBUSY when the queue is full, WAR_EINVAL for a bad job. */

@@ -53,6 +53,8 @@ def test_compute_entry_points_fail_without_device():
         warlib.enumerate_plain(warlib.make_job(9))
     with pytest.raises(warlib.WarError):
         warlib.floyd_sample(warlib.make_job(9, flags=warlib.F_SAMPLE, sample_ppm=1000))
+    with pytest.raises(warlib.WarError):
+        warlib.autotune_native(warlib.make_job(9))
 
 
 def test_argument_errors():

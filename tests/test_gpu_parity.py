@@ -146,3 +146,12 @@ def test_n14_canon_full(wl, golden):
     assert (f.s_count, f.s_cyc, f.s_lamsum, f.s_lensum, f.s_maxfin) == \
         (r["s_count"], r["s_cyc"], r["s_lamsum"], r["s_lensum"], r["s_maxfin"])
     assert 0.009 * g["positions"] < r["s_count"] < 0.011 * g["positions"]
+
+
+def test_native_autotune_keeps_counts(wl, oracle):
+    """war_autotune searches on a slice and returns a tune whose full-job counts equal the oracle's."""
+    job = wl.make_job(11, hbins=64)
+    best, ms = wl.autotune_native(job, slice_ms=30.0, passes=1)
+    assert ms > 0 and best.threads in (128, 256, 512, 1024)
+    want = oracle.enumerate_job(ojob(oracle, job))
+    same(wl, oracle, wl.enumerate_job(job, best), want)

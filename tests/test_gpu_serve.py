@@ -72,3 +72,19 @@ def test_poisson_stream_small(wl):
     assert all(r is not None for r in results)
     assert serve.verify(stream[:40], results[:40]) == 0
     assert serve.percentile(lat, 50) <= serve.percentile(lat, 99)
+
+
+def test_shared_memo_same_as_without(wl):
+    """Jobs of one n and rule share the server's cycle memo; the results equal a server without it, and a
+    memo far too small for the class changes nothing either."""
+    import serve
+    jobs = mix(wl) + [wl.make_job(13, lo=10 ** 9, hi=10 ** 9 + 2 * 10 ** 7, hbins=128),
+                      wl.make_job(13, lo=10 ** 9 + 5, hi=10 ** 9 + 10 ** 7, hbins=128)]
+    got = {}
+    for bits in (0, -1, 12):
+        with serve.Server(memo_bits=bits) as s:
+            ids = [s.submit(j) for j in jobs]
+            got[bits] = [r for r, _ in s.wait_all(ids)]
+    for a, b, c in zip(got[0], got[-1], got[12]):
+        same(wl, a, b)
+        same(wl, c, b)
