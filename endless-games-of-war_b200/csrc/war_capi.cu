@@ -464,7 +464,72 @@ int war_enumerate_plain(const war_job* job, war_result* out) {
     return WAR_OK;
 }
 
+int war_enumerate_held(const war_job* job, const war_tune* tune, war_result* out) {
+    if (!job) return fail(WAR_EINVAL, "job is NULL");
+    if (!out) return fail(WAR_EINVAL, "out is NULL");
+    if (job->mode != WAR_DEALS || job->n < 2 || job->n > 17)
+        return fail(WAR_EINVAL, "the held-out engine plays deals of 2..17 cards (n=%d, mode=%d)", job->n, job->mode);
+    if (job->rule != 0 && job->rule != 1) return fail(WAR_EINVAL, "rule=%d", job->rule);
+    if (job->flags & ~WAR_F_MEMO_KEEP) return fail(WAR_EINVAL, "flags=0x%x: none apply to the held-out engine", job->flags);
+    if (job->hbins < 0 || job->hbins > WAR_HBINS_MAX) return fail(WAR_EINVAL, "hbins=%d", job->hbins);
+    if (job->lo > job->hi || job->hi > fact(job->n))
+        return fail(WAR_EINVAL, "range [%llu, %llu) outside the %d! deals", (unsigned long long)job->lo,
+                    (unsigned long long)job->hi, job->n);
+    memset(out, 0, sizeof *out);
+    out->hbins = job->hbins;
+    if (job->lo == job->hi) return WAR_OK;
+    int st;
+    if ((st = ensure_ready())) return st;
+    const int threads = (tune && tune->threads) ? tune->threads : 256;
+    const int block_m = std::min(job->n, (tune && tune->block_m) ? tune->block_m : 6);
+    const int W = (tune && tune->window) ? tune->window : 32;
+    const int defer = (tune && tune->defer) ? tune->defer : 16;
+    if (threads < 64 || threads > 1024 || (threads & 31)) return fail(WAR_EINVAL, "tune.threads=%d", threads);
+    if (block_m < 1 || block_m > 8) return fail(WAR_EINVAL, "tune.block_m=%d (1..8)", block_m);
+    if (W < 1 || W > (1 << 16) || (W & (W - 1))) return fail(WAR_EINVAL, "tune.window=%d", W);
+    if (defer < 1 || defer > 32) return fail(WAR_EINVAL, "tune.defer=%d (1..32)", defer);
+    const int maxb = held_max_blocks_per_sm(job->rule, threads, job->hbins);
+    if (maxb < 1) return fail(WAR_EINVAL, "launch shape threads=%d does not fit an SM", threads);
+    const int bps = (tune && tune->blocks_per_sm) ? std::min(tune->blocks_per_sm, maxb) : maxb;
+    std::lock_guard<std::mutex> lk(ctx().mu);
+    Ctx& c = ctx();
+    Plan p;
+    make_plan(job, block_m, p);
+    if (p.extra.size() > Ctx::UNIT_CAP) return fail(WAR_EINVAL, "plan has %zu extra units", p.extra.size());
+    cudaError_t e;
+    if (!p.extra.empty() &&
+        (e = cudaMemcpyAsync(c.d_units, p.extra.data(), sizeof(Unit) * p.extra.size(), cudaMemcpyHostToDevice,
+                             cur_stream())) != cudaSuccess)
+        return cuda_fail(e, "copy units");
+    HeldArgs a;
+    memset(&a, 0, sizeof a);
+    for (int i = 0; i <= 17; i++) a.fact[i] = fact(i);
+    a.n = job->n; a.m = block_m; a.rule = job->rule; a.hbins = job->hbins; a.W = W; a.defer = defer;
+    a.units = c.d_units;
+    // each launch plays fewer than 2^32 - 2^24 games (32-bit per-lane counters)
+    const u64 per_unit = fact(block_m);
+    const u64 max_units = std::max<u64>(1, ((1ull << 32) - (1ull << 24)) / per_unit);
+    u64 done_main = 0;
+    bool extras_done = p.extra.empty();
+    while (done_main < p.main_count || !extras_done) {
+        const u64 take = std::min<u64>(max_units, p.main_count - done_main);
+        const bool last = done_main + take >= p.main_count;
+        a.main_base = p.main_base + done_main;
+        a.main_count = take;
+        a.n_units = take + (last ? p.extra.size() : 0);
+        st = run_launch([&](cudaStream_t x) { return launch_held(a, threads, bps * c.sm_count, c.d_acc, x); },
+                        &out->kernel_ms);
+        if (st) return st;
+        merge_acc(*c.h_acc, out, job->hbins, 0);
+        out->units += a.n_units;
+        done_main += take;
+        if (last) extras_done = true;
+    }
+    return WAR_OK;
+}
+
 int war_enumerate(const war_job* job, const war_tune* tune, war_result* out) {
+    if (job && job->n == 17 && job->mode == WAR_DEALS) return war_enumerate_held(job, tune, out);   // 17 cards
     int st = check_job(job);
     if (st) return st;
     if (!out) return fail(WAR_EINVAL, "out is NULL");

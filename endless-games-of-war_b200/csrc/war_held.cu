@@ -1,0 +1,243 @@
+// war_held.cu — the held-out-card engine (war_enumerate_held): deals of up to 17 cards.
+//
+// With 17 cards a pile no longer fits 4-bit cards in one 64-bit word.  As gpu/war17.py:7-16 observes,
+// card n-1 never loses, so it never changes hands and its holder never runs out of cards: it can be kept
+// out of the packed piles.  The state is the holder's other cards wh (lh of them), the opponent's cards
+// wo (lo), and the depth p of card n-1 in the holder's full pile (0 = on top); lh + lo = n - 1, so
+// (wh, wo, lh, p) is the whole position and Brent compares exactly that (gpu/war17.py:62-71).  The game
+// ends when the opponent has no card.
+//
+// The kernel is the refill design of war_refill.cuh for this state: a persistent grid, one game per lane,
+// outcomes latched every turn and recorded every `defer` turns by the whole warp, work units of aligned
+// lexicographic rank blocks (fixed prefix, every order of the last j positions) from one global counter.
+// A unit is enumerated as (position of card n-1, order of the other cards): the others stay in deck order
+// in one word (16 nibbles at n = 17) and a unit permutes either the last j of them (card n-1 in the
+// prefix) or the last j-1 of them for each of the j positions of card n-1 in the suffix — the same set of
+// deals as the lexicographic block, so the counts are the same.
+#include "war_kernels.cuh"
+
+namespace war {
+
+__device__ __forceinline__ u64 shr64(u64 x, u32 s) {   // PTX shr: amounts above 63 give 0
+    u64 r;
+    asm("shr.b64 %0, %1, %2;" : "=l"(r) : "l"(x), "r"(s));
+    return r;
+}
+
+__device__ __forceinline__ u32 h_heap_full(u32 j) {
+    u32 f = 0;
+    for (u32 i = 1; i < j; i++) f |= i << (4u * i);
+    return f;
+}
+
+struct HEnum {
+    u64 O;             // the cards other than n-1, in deck order (others index i in nibble i)
+    u32 pos, pos_end;  // position of card n-1 in the deck; positions still to take it: [pos, pos_end)
+    u32 base, J;       // Heap's algorithm permutes others indices [base, base + J)
+    u32 ctr, full;     // Heap counter (digit i in nibble i) and its last value
+    bool live;         // (O, pos) is the next unplayed deal
+};
+
+// Takes the next unit; false when there is none.  Unranks its first (lexicographic) order.
+__device__ __forceinline__ bool h_fetch(HEnum& E, const HeldArgs& a, u64* counter) {
+    const u64 u = atomicAdd(counter, 1ull);
+    if (u >= a.n_units) return false;
+    u64 r;
+    u32 j;
+    if (u < a.main_count) {
+        j = (u32)a.m;
+        r = (a.main_base + u) * a.fact[a.m];
+    } else {
+        const Unit U = a.units[u - a.main_count];
+        r = U.r;
+        j = U.j;
+    }
+    const u32 n = (u32)a.n;
+    u32 avail = (1u << n) - 1u, cnt = 0, pos = 0;
+    u64 O = 0;
+    for (u32 i = 0; i < n; i++) {   // lexicographic unrank (gpu/war17.py:95-104)
+        const u64 f = a.fact[n - 1u - i];
+        const u32 d = (u32)(r / f);
+        r -= (u64)d * f;
+        u32 mm = avail;
+        for (u32 k = 0; k < d; k++) mm &= mm - 1u;
+        const u32 v = (u32)(__ffs((int)mm) - 1);
+        avail &= ~(1u << v);
+        if (v == n - 1u) pos = i;
+        else { O |= (u64)v << (4u * cnt); cnt++; }
+    }
+    const u32 b = n - j;   // first permuted deck position
+    E.O = O;
+    if (pos < b) { E.pos = pos; E.pos_end = pos + 1u; E.base = b - 1u; E.J = j; }
+    else { E.pos = b; E.pos_end = n; E.base = b; E.J = j - 1u; }
+    E.ctr = 0;
+    E.full = h_heap_full(E.J);
+    E.live = true;
+    return true;
+}
+
+// Advances to the next deal of the unit (Heap's algorithm over the J permuted others; when it has run
+// through all their orders, card n-1 moves one position further).  False after the unit's last deal.
+__device__ __forceinline__ bool h_step(HEnum& E) {
+    const u32 x = E.ctr ^ E.full;
+    if (x != 0u) {
+        const u32 i = (u32)(__ffs((int)x) - 1) >> 2;
+        const u32 ci = (E.ctr >> (4u * i)) & 15u;
+        const u32 o = (i & 1u) ? ci : 0u;
+        const u32 sa = 4u * (E.base + i), sb = 4u * (E.base + o);
+        const u64 t = ((E.O >> sa) ^ (E.O >> sb)) & 15ull;
+        E.O ^= (t << sa) | (t << sb);
+        E.ctr = ((E.ctr >> (4u * i)) + 1u) << (4u * i);
+        return true;
+    }
+    if (E.pos + 1u < E.pos_end) {   // every order of the others seen: next position of card n-1
+        E.pos++;
+        E.ctr = 0;
+        return true;
+    }
+    return false;
+}
+
+// Player 1 gets the even deck positions, player 2 the odd ones, the first card on top (gpu/war17.py:48-60).
+__device__ __forceinline__ void h_deal(u64 O, u32 pos, u32 n, u64& wh, u64& wo, u32& lh, u32& lo, u32& p) {
+    const u32 L = pos;                                   // others dealt before card n-1
+    const u64 low = L ? (O & (shr64(~0ull, 64u - 4u * L))) : 0ull;
+    const u64 high = shr64(O, 4u * L);
+    const u64 p1l = compact_even_nibbles(low), p2l = compact_even_nibbles(low >> 4);
+    // after card n-1 the deck position of others index i is i + 1, so the parities swap
+    const u64 he = compact_even_nibbles(high), ho = compact_even_nibbles(high >> 4);
+    const u64 p1h = (L & 1u) ? he : ho, p2h = (L & 1u) ? ho : he;
+    const u64 p1 = p1l | (p1h << (4u * ((L + 1u) >> 1))), p2 = p2l | (p2h << (4u * (L >> 1)));
+    const u32 n1 = (n + 1u) >> 1, n2 = n >> 1;
+    const bool h1 = (pos & 1u) == 0u;                    // player 1 holds card n-1
+    wh = h1 ? p1 : p2;
+    wo = h1 ? p2 : p1;
+    lh = h1 ? n1 - 1u : n2 - 1u;
+    lo = h1 ? n2 : n1;
+    p = pos >> 1;
+}
+
+// One turn (gpu/war17.py:36-47, with the put-back order of rule 1 added).  Returns true when the game
+// is over (the opponent has no card).
+template <int RULE>
+__device__ __forceinline__ bool h_turn(u64& wh, u64& wo, u32& lh, u32& lo, u32& p) {
+    const u32 c = (u32)wo & 15u;
+    wo >>= 4;
+    lo--;
+    if (p == 0u) {   // the holder plays card n-1 and wins the opponent's card
+        wh |= shl64((u64)c, 4u * lh);
+        lh++;
+        p = RULE ? lh : lh - 1u;   // rule 0: n-1 above the captured card; rule 1: below it
+    } else {
+        const u32 h = (u32)wh & 15u;
+        wh >>= 4;
+        lh--;
+        p--;
+        const u32 hi = max(h, c), lw = min(h, c);
+        const u32 pair = RULE ? (lw | (hi << 4)) : (hi | (lw << 4));
+        if (h > c) { wh |= shl64((u64)pair, 4u * lh); lh += 2u; }
+        else { wo |= shl64((u64)pair, 4u * lo); lo += 2u; }
+    }
+    return lo == 0u;
+}
+
+template <int RULE>
+__global__ void __launch_bounds__(1024) held_kernel(const __grid_constant__ HeldArgs a, DevAcc* __restrict__ acc) {
+    extern __shared__ u32 sh[];
+    u32* shh = sh;
+    u32* she = sh + a.hbins;
+    for (int b = threadIdx.x; b < a.hbins + WAR_EBINS; b += blockDim.x) sh[b] = 0;
+    __syncthreads();
+
+    const u32 n = (u32)a.n, W = (u32)a.W;
+    const u32 hb1 = a.hbins > 0 ? (u32)(a.hbins - 1) : 0u;
+    const int period = a.defer > 4 ? (a.defer + 3) & ~3 : 4;
+    u64* counter = &acc->work_next;
+
+    HEnum E;
+    E.live = false;
+    u64 wh = 0, wo = 0, th = 0, to = 0;
+    u32 lh = 0, lo = 0, p = 0, tlh = 0, tp = 0, rounds = 0, next = 0;
+    bool done = true, kcy = false, active = false;
+    u32 cyc = 0, ndone = 0, maxfin = 0, capped = 0, turns = 0;
+
+    auto start_game = [&]() {
+        active = false;
+        for (;;) {
+            if (!E.live && !h_fetch(E, a, counter)) return;
+            h_deal(E.O, E.pos, n, wh, wo, lh, lo, p);
+            E.live = h_step(E);
+            break;
+        }
+        active = true;
+        ndone++;
+        th = wh; to = wo; tlh = lh; tp = p;
+        rounds = 0; next = W; kcy = false;
+        done = lo == 0u;   // n = 1 only (never here: n >= 2)
+    };
+
+    start_game();
+    bool running = __any_sync(WAR_FULL_MASK, active);
+    while (running) {
+        for (int k = 0; k < period; k++) {
+            bool en = h_turn<RULE>(wh, wo, lh, lo, p);
+            if (!done) rounds++;
+            const bool cy = (wh == th) & (wo == to) & (lh == tlh) & (p == tp);
+            en = en | (lo == 0u);
+            const bool fin = (cy | en) & !done;
+            kcy = fin ? (cy & !en) : kcy;
+            done = done | fin;
+            if (lo == 0u) { lo = 1u; wo = 0ull; }   // a finished game keeps being stepped harmlessly
+            if (rounds == next && !done) {
+                if (next > WAR_TURN_CAP) { capped++; done = true; active = false; }
+                else { th = wh; to = wo; tlh = lh; tp = p; next = 2u * next + W; }
+            }
+        }
+        if (__any_sync(WAR_FULL_MASK, done & active)) {
+            if (done & active) {
+                turns += rounds;
+                if (kcy) {
+                    const u32 lam = rounds - ((next - W) >> 1);
+                    cyc++;
+                    if (a.hbins) atomicAdd(&shh[lam < hb1 ? lam : hb1], 1u);
+                } else {
+                    if (rounds > maxfin) maxfin = rounds;
+                    atomicAdd(&she[rounds < WAR_EBINS - 1 ? rounds : WAR_EBINS - 1], 1u);
+                }
+                start_game();
+            }
+            running = __any_sync(WAR_FULL_MASK, active);
+        }
+    }
+
+    const u64 v_cyc = warp_sum(cyc), v_done = warp_sum(ndone), v_turns = warp_sum((u64)turns), v_max = warp_max(maxfin);
+    const u64 v_cap = warp_sum(capped);
+    if ((threadIdx.x & 31) == 0) {
+        if (v_cyc) atomicAdd(&acc->cyc, v_cyc);
+        if (v_done) atomicAdd(&acc->done, v_done);
+        if (v_turns) atomicAdd(&acc->turns, v_turns);
+        if (v_max) atomicMax(&acc->maxfin, v_max);
+        if (v_cap) atomicAdd(&acc->status, v_cap);
+    }
+    __syncthreads();
+    flush_hist(shh, acc->hist, a.hbins);
+    flush_hist(she, acc->endhist, WAR_EBINS);
+}
+
+cudaError_t launch_held(const HeldArgs& a, int threads, int blocks, DevAcc* acc, cudaStream_t st) {
+    const size_t shmem = sizeof(u32) * (size_t)(a.hbins + WAR_EBINS);
+    if (a.rule) held_kernel<1><<<blocks, threads, shmem, st>>>(a, acc);
+    else held_kernel<0><<<blocks, threads, shmem, st>>>(a, acc);
+    note_launch();
+    return cudaGetLastError();
+}
+
+int held_max_blocks_per_sm(int rule, int threads, int hbins) {
+    int nb = 0;
+    const size_t shmem = sizeof(u32) * (size_t)(hbins + WAR_EBINS);
+    cudaError_t e = rule ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, held_kernel<1>, threads, shmem)
+                         : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, held_kernel<0>, threads, shmem);
+    return e == cudaSuccess ? nb : 0;
+}
+
+}  // namespace war

@@ -129,6 +129,16 @@ cudaError_t launch_batched(const BatchArgs& a, int canon, int rule, int shape, c
 int batched_max_blocks_per_sm(int canon, int rule, int shape, int distinct, int sample, int threads, int games,
                               int hbins, int variant);
 
+// Held-out-card engine (war_held.cu): deals of n <= 17 cards.
+struct HeldArgs {
+    u64 fact[18];
+    u64 main_base, main_count, n_units;   // as in BatchArgs
+    const Unit* units;
+    int n, m, rule, hbins, W, defer;
+};
+cudaError_t launch_held(const HeldArgs& a, int threads, int blocks, DevAcc* acc, cudaStream_t st);
+int held_max_blocks_per_sm(int rule, int threads, int hbins);
+
 struct FloydArgs {
     u64 fact[17];
     u64 start, total;       // rank range (deals: deal ranks; canon: position ranks)

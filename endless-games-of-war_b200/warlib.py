@@ -86,6 +86,7 @@ SYMBOLS = {
                                         ctypes.c_int32, U64P, ctypes.c_int32]),
     "war_enumerate_plain": (ctypes.c_int, [ctypes.POINTER(Job), ctypes.POINTER(Result)]),
     "war_enumerate": (ctypes.c_int, [ctypes.POINTER(Job), ctypes.POINTER(Tune), ctypes.POINTER(Result)]),
+    "war_enumerate_held": (ctypes.c_int, [ctypes.POINTER(Job), ctypes.POINTER(Tune), ctypes.POINTER(Result)]),
     "war_floyd_sample": (ctypes.c_int, [ctypes.POINTER(Job), ctypes.POINTER(Result)]),
     "war_enumerate_noalloc": (ctypes.c_int, [ctypes.POINTER(Job), ctypes.POINTER(Tune), ctypes.POINTER(Result)]),
     "war_autotune": (ctypes.c_int, [ctypes.POINTER(Job), ctypes.POINTER(Tune), ctypes.c_double, ctypes.c_int32,
@@ -166,6 +167,14 @@ def autotune_native(job, start=None, slice_ms=400.0, passes=2):
     check(lib().war_autotune(ctypes.byref(job), ctypes.byref(start) if start is not None else None, slice_ms, passes,
                              ctypes.byref(best), ctypes.byref(ms)), "war_autotune")
     return best, ms.value
+
+
+def enumerate_held(job, tune=None):
+    """war_enumerate_held: deals of up to 17 cards with the held-out-card engine."""
+    r = Result()
+    check(lib().war_enumerate_held(ctypes.byref(job), ctypes.byref(tune) if tune is not None else None,
+                                   ctypes.byref(r)), "war_enumerate_held")
+    return r
 
 
 def enumerate_noalloc(job, tune=None):

@@ -13,7 +13,8 @@
  * (war_server_*) runs its own host thread.
  *
  * Card values are 0..n-1 (0 lowest), deck position 0,2,4,.. goes to player 1 and 1,3,5,.. to
- * player 2, the first card dealt on top, as in gpu/war_gpu.py:3-5.  1 <= n <= 16.
+ * player 2, the first card dealt on top, as in gpu/war_gpu.py:3-5.  1 <= n <= 16 (deals: 17, see
+ * war_enumerate_held).
  */
 #ifndef WAR_B200_WAR_H
 #define WAR_B200_WAR_H
@@ -186,6 +187,14 @@ typedef struct war_job_status {
     int32_t status;          /* war_status of a failed job */
     double submit_ms, admit_ms, finish_ms; /* host clock (ms since the server started) */
 } war_job_status;
+
+/* Deals of 2..17 cards with the held-out-card engine (gpu/war17.py:7-16, :36-71): card n-1 never loses,
+ * so it is kept out of the packed piles and tracked by its depth in its holder's pile; that keeps 17
+ * cards in 4-bit nibbles.  Same job and result as war_enumerate for deals (cycling count, longest ending
+ * game, cycle-length and ending-length histograms, turns), both rules; no flags apply (the memo does not:
+ * a 17-card position is wider than a memo key).  tune: threads, blocks_per_sm, block_m, window and defer
+ * are used, the rest ignored; NULL = defaults.  war_enumerate sends n = 17 deal jobs here. */
+int war_enumerate_held(const war_job* job, const war_tune* tune, war_result* out);
 
 /* Coordinate descent over war_tune for the class of `job` (block_m, games, threads, blocks per SM, window,
  * defer, variant, memo_bits), timed by war_enumerate's kernel time on a slice of job's range from its

@@ -58,6 +58,7 @@ def lib():
         _lib = ctypes.CDLL(path)
         _lib.oracle_enumerate.argtypes = [ctypes.POINTER(Job), ctypes.c_int, ctypes.POINTER(Result)]
         _lib.oracle_floyd_sample.argtypes = [ctypes.POINTER(Job), ctypes.c_int, ctypes.POINTER(Result)]
+        _lib.oracle_enumerate_held.argtypes = [ctypes.POINTER(Job), ctypes.c_int, ctypes.POINTER(Result)]
         _lib.oracle_play_one.argtypes = [ctypes.c_uint64, ctypes.c_int, ctypes.c_uint64, ctypes.c_int,
                                          ctypes.c_int, ctypes.POINTER(ctypes.c_uint64),
                                          ctypes.POINTER(ctypes.c_uint64)]
@@ -95,6 +96,15 @@ def enumerate_job(job, threads=0):
     st = lib().oracle_enumerate(ctypes.byref(job), threads, ctypes.byref(r))
     if st != 0:
         raise ValueError("oracle_enumerate: status %d" % st)
+    return r
+
+
+def enumerate_held(job, threads=0):
+    """The held-out-card program of gpu/war17.py on ranks [lo, hi) of the n! deals (n <= 17)."""
+    r = Result()
+    st = lib().oracle_enumerate_held(ctypes.byref(job), threads, ctypes.byref(r))
+    if st != 0:
+        raise ValueError("oracle_enumerate_held: status %d" % st)
     return r
 
 

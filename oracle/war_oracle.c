@@ -14,6 +14,7 @@
  *   min-key distinct  distinct_cycles     cpu/distinct_cycles.c:84-92, :128-141
  *   loop_shape        Theorem-3 test      gpu/war_gpu.py:51-73
  *   floyd             second detector     gpu/war_gpu_floyd.py:95-105 (tortoise/hare, hare steps = game length)
+ *   held-out card     n <= 17 deals       gpu/war17.py:36-113 (oracle_enumerate_held)
  * Piles use the reference's layout: 4-bit cards in a uint64, top card in the low nibble, explicit
  * lengths.  Additions with no reference counterpart (turn totals, ending-length histogram, sample
  * aggregates) are computed from the same per-game results.
@@ -356,6 +357,124 @@ int oracle_play_one(uint64_t w1, int l1, uint64_t w2, int l2, int rule, uint64_t
     St s; s.w1 = w1; s.w2 = w2; s.l1 = l1; s.l2 = l2;
     *lam = 0;
     return brent(s, rule, rounds, lam, NULL);
+}
+
+/* ---- the held-out-card program, gpu/war17.py (deals of n <= 17) -------------------------------------
+ * Card n-1 is kept out of the packed piles (gpu/war17.py:7-16); the holder's other cards, the opponent's
+ * cards and the depth p of card n-1 in the holder's pile are the state; Brent on the whole state with the
+ * reference's schedule (:62-71).  Rule 1 (loser's card first) is added the same way as in war_gpu.py. */
+typedef struct { uint64_t wh, wo; int lh, lo, p; } HSt;
+
+/* turn, gpu/war17.py:36-47.  Returns 1 when the opponent is out of cards. */
+static inline int hturn(HSt* s, int rule) {
+    if (s->p == 0) {
+        uint64_t c = s->wo & 15u; s->wo >>= 4; s->lo--;
+        if (rule) { s->wh |= c << (4 * s->lh); s->lh++; s->p = s->lh; }
+        else { s->p = s->lh; s->wh |= c << (4 * s->lh); s->lh++; }
+        return s->lo == 0;
+    }
+    uint64_t h = s->wh & 15u; s->wh >>= 4; s->lh--; s->p--;
+    uint64_t o = s->wo & 15u; s->wo >>= 4; s->lo--;
+    if (h > o) {
+        uint64_t x = rule ? o : h, y = rule ? h : o;
+        s->wh |= x << (4 * s->lh); s->lh++; s->wh |= y << (4 * s->lh); s->lh++;
+    } else {
+        uint64_t x = rule ? h : o, y = rule ? o : h;
+        s->wo |= x << (4 * s->lo); s->lo++; s->wo |= y << (4 * s->lo); s->lo++;
+    }
+    return s->lo == 0;
+}
+
+/* deal_cycles, gpu/war17.py:50-71.  Returns 1 if the game never ends; *len = turns to the end, or the
+ * turns played until the repeat was found; *lam = the cycle length. */
+static int hdeal(const unsigned char* a, int n, int rule, uint64_t* len, uint64_t* lam_out) {
+    uint64_t w1 = 0, w2 = 0; int l1 = 0, l2 = 0, holder = 0, p = 0;
+    for (int i = 0; i < n; i++) {
+        int pl = i & 1;
+        if (a[i] == (unsigned char)(n - 1)) { holder = pl; p = pl ? l2 : l1; continue; }
+        if (pl == 0) { w1 |= ((uint64_t)a[i]) << (4 * l1); l1++; }
+        else { w2 |= ((uint64_t)a[i]) << (4 * l2); l2++; }
+    }
+    HSt s; s.wh = holder ? w2 : w1; s.wo = holder ? w1 : w2; s.lh = holder ? l2 : l1; s.lo = holder ? l1 : l2; s.p = p;
+    if (s.lo == 0) { *len = 0; return 0; }
+    HSt t = s;
+    uint64_t power = 1, lam = 0, rounds = 0;
+    for (;;) {
+        rounds++;
+        if (hturn(&s, rule)) { *len = rounds; return 0; }
+        lam++;
+        if (s.wh == t.wh && s.wo == t.wo && s.lh == t.lh && s.p == t.p) { *len = rounds; *lam_out = lam; return 1; }
+        if (lam == power) { t = s; power <<= 1; lam = 0; }
+    }
+}
+
+/* Ranks [lo, hi) of the n! deals (lexicographic, gpu/war17.py:95-113) with the held-out program. */
+int oracle_enumerate_held(const war_job* job, int nthreads, war_result* out) {
+    if (!job || !out || job->n < 2 || job->n > 17 || job->mode != WAR_DEALS) return WAR_EINVAL;
+    if (job->hbins < 0 || job->hbins > WAR_HBINS_MAX) return WAR_EINVAL;
+    const int n = job->n, rule = job->rule, hbins = job->hbins;
+    uint64_t f[18]; f[0] = 1;
+    for (int i = 1; i <= 17; i++) f[i] = f[i - 1] * (uint64_t)i;
+    if (job->lo > job->hi || job->hi > f[n]) return WAR_EINVAL;
+    memset(out, 0, sizeof(*out));
+    out->hbins = hbins;
+#ifdef _OPENMP
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+#else
+    nthreads = 1;
+#endif
+    uint64_t len = job->hi - job->lo;
+    if ((uint64_t)nthreads > len / 64 + 1) nthreads = (int)(len / 64 + 1);
+    war_result* parts = (war_result*)calloc((size_t)nthreads, sizeof(war_result));
+    if (!parts) return WAR_ENOMEM;
+    uint64_t pieces = (uint64_t)nthreads * 64u;
+    if (pieces > len) pieces = len ? len : 1;
+    #pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
+    for (long long pc = 0; pc < (long long)pieces; pc++) {
+        int tid = 0;
+#ifdef _OPENMP
+        tid = omp_get_thread_num();
+#endif
+        war_result* acc = &parts[tid];
+        uint64_t lo = job->lo + len * (uint64_t)pc / pieces, hi = job->lo + len * (uint64_t)(pc + 1) / pieces;
+        if (lo >= hi) continue;
+        unsigned char a[17];
+        unsigned avail = (1u << n) - 1u;
+        uint64_t r = lo;
+        for (int i = 0; i < n; i++) {
+            uint64_t fi = f[n - 1 - i];
+            int d = (int)(r / fi); r -= (uint64_t)d * fi;
+            unsigned m = avail;
+            for (int k = 0; k < d; k++) m &= m - 1u;
+            int v = __builtin_ctz(m);
+            a[i] = (unsigned char)v; avail &= ~(1u << v);
+        }
+        for (uint64_t q = lo; q < hi; q++) {
+            uint64_t gl = 0, lam = 0;
+            acc->done++;
+            if (hdeal(a, n, rule, &gl, &lam)) {
+                acc->cyc++;
+                if (hbins) acc->hist[lam < (uint64_t)(hbins - 1) ? lam : (uint64_t)(hbins - 1)]++;
+            } else {
+                if (gl > acc->maxfin) acc->maxfin = gl;
+                acc->endhist[gl < WAR_EBINS - 1 ? gl : WAR_EBINS - 1]++;
+            }
+            acc->turns += gl;
+            if (q + 1 < hi) {   /* next_perm, gpu/war17.py:74-84 */
+                int i = n - 2;
+                while (i >= 0 && a[i] >= a[i + 1]) i--;
+                if (i >= 0) {
+                    int j = n - 1;
+                    while (a[j] <= a[i]) j--;
+                    unsigned char t = a[i]; a[i] = a[j]; a[j] = t;
+                    for (int l = i + 1, rr = n - 1; l < rr; l++, rr--) { t = a[l]; a[l] = a[rr]; a[rr] = t; }
+                }
+            }
+        }
+    }
+    for (int t = 0; t < nthreads; t++) merge(out, &parts[t]);
+    free(parts);
+    return WAR_OK;
 }
 
 uint64_t oracle_space_size(int n, int mode) { return space_size(n, mode); }

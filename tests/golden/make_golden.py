@@ -120,6 +120,8 @@ def main():
         "deals_hist256": out_lines(checks.split("== Deals, n = 1..13")[1].split("==")[0]),
         "canon_distinct_shape": out_lines(
             checks.split("== Canonical positions, distinct cycles and the Theorem-3 test, n = 1..13")[1].split("==")[0]),
+        # gpu/war17.py 13 --nmin 5 (checks.txt:81-91)
+        "war17_5_13": out_lines(checks.split("== Deals, 17-card GPU program")[1].split("==")[0]),
     }
 
     # n = 14, 15 long deal runs with histograms (long_runs.txt:13-17)

@@ -1,0 +1,84 @@
+"""The held-out-card engine (war_enumerate_held, the n <= 17 program gpu/war17.py): bit-exact against the
+oracle's restatement of gpu/war17.py and against the main engine where both apply, and against the
+recorded a(12), a(13) and histogram."""
+import random
+
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("cyc", "done", "maxfin", "hist", "endhist")
+
+
+def held(wl, n, rule=0, lo=0, hi=None, hbins=128, tune=None):
+    return wl.to_dict(wl.enumerate_held(wl.make_job(n, rule=rule, lo=lo, hi=hi, hbins=hbins), tune))
+
+
+def oracle_held(oracle, n, rule=0, lo=0, hi=None, hbins=128):
+    import math
+    hi = math.factorial(n) if hi is None else hi
+    return oracle.to_dict(oracle.enumerate_held(oracle.make_job(n, 0, rule, 0, lo, hi, hbins)))
+
+
+@pytest.mark.parametrize("rule", [0, 1])
+def test_small_n_full_against_oracle_and_main_engine(wl, oracle, rule):
+    for n in range(2, 12):
+        got = held(wl, n, rule)
+        want = oracle_held(oracle, n, rule)
+        main = wl.to_dict(wl.enumerate_job(wl.make_job(n, rule=rule, hbins=128)))
+        for k in FIELDS:
+            assert got[k] == want[k] == main[k], (n, rule, k)
+
+
+def test_a12_a13_recorded(wl, golden):
+    for n in (12, 13):
+        r = held(wl, n, hbins=256)
+        g = golden["deals_rule0"][n]
+        assert (r["done"], r["cyc"], r["maxfin"], r["hist"]) == (g["deals"], g["cyc"], g["longest"], g["hist"])
+
+
+@pytest.mark.parametrize("n", [14, 15, 16, 17])
+def test_slices_against_oracle(wl, oracle, n):
+    import math
+    rnd = random.Random(n)
+    total = math.factorial(n)
+    for _ in range(4):
+        lo = rnd.randrange(0, total)
+        hi = min(total, lo + rnd.choice([1, 5, 999, 40320, 300001]))
+        rule = rnd.randint(0, 1)
+        got, want = held(wl, n, rule, lo, hi, 256), oracle_held(oracle, n, rule, lo, hi, 256)
+        for k in FIELDS:
+            assert got[k] == want[k], (n, lo, hi, rule, k)
+    for lo in (0, total - 720 * 33 - 17):   # the first and the last deals of the space
+        got, want = held(wl, n, 0, lo, lo + 720 * 33 + 17, 256), oracle_held(oracle, n, 0, lo, lo + 720 * 33 + 17, 256)
+        for k in FIELDS:
+            assert got[k] == want[k], (n, lo, k)
+
+
+def test_n16_slice_against_main_engine(wl):
+    job = dict(lo=10 ** 13, hi=10 ** 13 + 5 * 10 ** 7, hbins=256)
+    got = held(wl, 16, **job)
+    main = wl.to_dict(wl.enumerate_plain(wl.make_job(16, **job)))
+    for k in FIELDS:
+        assert got[k] == main[k], k
+
+
+def test_n17_through_war_enumerate_and_tunes(wl, oracle):
+    lo, hi = 2 * 10 ** 14 + 12345, 2 * 10 ** 14 + 12345 + 250000
+    want = oracle_held(oracle, 17, 0, lo, hi, 256)
+    got = wl.to_dict(wl.enumerate_job(wl.make_job(17, lo=lo, hi=hi, hbins=256)))   # routed to the held engine
+    for k in FIELDS:
+        assert got[k] == want[k], k
+    for t in (dict(threads=128), dict(threads=1024, defer=4), dict(block_m=3, defer=16), dict(block_m=8, window=1),
+              dict(blocks_per_sm=1, window=128)):
+        got = held(wl, 17, 0, lo, hi, 256, wl.make_tune(**t))
+        for k in FIELDS:
+            assert got[k] == want[k], (t, k)
+
+
+def test_refusals(wl):
+    import warlib
+    for bad in (dict(n=1), dict(n=18), dict(n=9, mode=1), dict(n=9, flags=warlib.F_SAMPLE)):
+        job = wl.make_job(**bad)
+        with pytest.raises(warlib.WarError):
+            wl.enumerate_held(job)

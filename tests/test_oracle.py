@@ -141,3 +141,17 @@ def test_oracle_matches_reference_distinct_cycles(oracle):
         cycling, oncycle, distinct, lens = oracle.ref_distinct(n, 2)
         r = oracle.enumerate_job(oracle.make_job(n, mode=oracle.CANON, flags=oracle.F_DISTINCT, dbins=64))
         assert (r.cyc, r.oncycle, r.distinct_min) == (cycling, oncycle, distinct)
+
+
+@pytest.mark.parametrize("rule", [0, 1])
+def test_held_out_restatement_agrees(oracle, golden, rule):
+    """The restatement of gpu/war17.py (card n-1 held out of the piles) against the war_gpu.py restatement
+    for every deal of n <= 10, and against the recorded a(n) and longest game."""
+    for n in range(2, 11):
+        a = oracle.to_dict(oracle.enumerate_job(oracle.make_job(n, 0, rule, 0, 0, None, 128)))
+        b = oracle.to_dict(oracle.enumerate_held(oracle.make_job(n, 0, rule, 0, 0, None, 128)))
+        for k in ("cyc", "done", "maxfin", "hist", "endhist"):
+            assert a[k] == b[k], (n, rule, k)
+        if rule == 0:
+            g = golden["deals_rule0"][n]
+            assert (b["cyc"], b["done"], b["maxfin"]) == (g["cyc"], g["deals"], g["longest"])

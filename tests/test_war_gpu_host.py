@@ -96,3 +96,43 @@ def test_tune_override_fields(monkeypatch):
     assert (t.threads, t.variant, t.memo_bits) == (256, 31, 28)
     with pytest.raises(ValueError):
         war_gpu.override_tune(None, {"no_such_field": 1})
+
+
+TIME17 = re.compile(r"  [0-9.]+s  slowest launch [0-9.]+s")
+
+
+def test_war17_lines_match_the_recorded_output(monkeypatch, oracle, golden):
+    """`war17.py 11 --nmin 5` (data/checks.txt:81-91, n <= 11) with the oracle's gpu/war17.py restatement
+    standing in for the held-out engine."""
+    import warlib
+    import war17
+
+    def enum(job, tune=None):
+        return oracle.enumerate_held(oracle.make_job(job.n, job.mode, job.rule, 0, job.lo, job.hi, job.hbins))
+    monkeypatch.setattr(warlib, "enumerate_held", enum)
+    buf = io.StringIO()
+    with contextlib.redirect_stdout(buf):
+        war17.main(["11", "--nmin", "5"])
+    got = [TIME17.sub("  X", ln) for ln in buf.getvalue().splitlines()]
+    want = [TIME17.sub("  X", ln) for ln in golden["war_gpu_lines"]["war17_5_13"] if int(ln.split()[0][2:]) <= 11]
+    assert got == want
+
+
+def test_war17_resume(monkeypatch, oracle, tmp_path):
+    import warlib
+    import war17
+    calls = []
+
+    def enum(job, tune=None):
+        calls.append(job.lo)
+        if len(calls) == 3:
+            raise KeyboardInterrupt("interrupted by the test")
+        return oracle.enumerate_held(oracle.make_job(job.n, job.mode, job.rule, 0, job.lo, job.hi, job.hbins))
+    monkeypatch.setattr(warlib, "enumerate_held", enum)
+    monkeypatch.setattr(war17, "SPAN_RANKS", 50000)
+    out = str(tmp_path / "n9")
+    with pytest.raises(KeyboardInterrupt):
+        war17.run(9, per=4, batch_threads=256, out=out)
+    calls.append(None)   # no more interruptions
+    r = war17.run(9, per=4, batch_threads=256, out=out, resume=True)
+    assert r[:3] == (218680, 362880, 28)
