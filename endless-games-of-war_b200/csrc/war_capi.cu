@@ -210,11 +210,11 @@ int resolve_tune(const war_job* job, const war_tune* in, Tune& t) {
     if (t.defer < 1 || t.defer > 32) return fail(WAR_EINVAL, "tune.defer=%d (1..32)", t.defer);
     if (t.variant < 0 || t.variant > 31) return fail(WAR_EINVAL, "tune.variant=%d (0..31)", t.variant);
     if (t.memo_bits < 12 || t.memo_bits > 31) return fail(WAR_EINVAL, "tune.memo_bits=%d (12..31)", t.memo_bits);
-    // the cycle memo serves deals of 4..15 cards with latched records, all states up to 14 cards;
-    // canonical scans take the path memo only
-    if ((t.variant & 4) && (!(t.variant & 2) || job->n < 4 || job->n > 15)) t.variant &= 3;
+    // the cycle memo needs latched records and n >= 4; its landmark form serves n <= 15, the all-states
+    // form n <= 14, the path form n <= 16; canonical scans take the path form only
+    const int memo_nmax = (t.variant & 28) == 28 ? 16 : ((t.variant & 8) ? 14 : 15);
+    if ((t.variant & 4) && (!(t.variant & 2) || job->n < 4 || job->n > memo_nmax)) t.variant &= 3;
     if (canon && !(t.variant & 16)) t.variant &= 3;
-    if ((t.variant & 8) && job->n > 14) t.variant &= 7;
     if (!(t.variant & 4)) t.variant &= 7;
     if (!(t.variant & 8)) t.variant &= 15;
     const int M = canon ? job->n - 1 : job->n;

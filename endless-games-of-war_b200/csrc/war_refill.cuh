@@ -377,7 +377,7 @@ __device__ __forceinline__ u64 memo_key(u64 h, u64 o, u32 n) {
 }
 
 __device__ __forceinline__ u32 memo_slot(u64 key, u32 bits) {
-    return (u32)((key * 0x9E3779B97F4A7C15ull) >> (64u - bits));
+    return (u32)((key * 0x9E3779B97F4A7C15ull) >> (64u - bits));   // the multiplier of path_entry
 }
 
 // The atomic is skipped when the slot already holds this entry or a larger one (it would change
@@ -400,7 +400,17 @@ __device__ __forceinline__ void memo_put(u64* T, u32 bits, u64 key, u32 lsh, u32
 // after a few turns, so a later game is decided where it meets such a state.  All entries of these two
 // memos are plain fire-and-forget stores that overwrite the slot (the most recent paths are the useful
 // ones; an aligned 8-byte store never tears, and a lost entry only means a later decision).
+//
+// A path-memo entry does not hold its key.  H = key * C is a bijection of 64-bit words (C odd); the slot
+// is the top `bits` bits of H and the entry holds the other 64 - bits bits of H above a value of `bits`
+// bits, (H << bits) | value.  Slot and entry together give back H, hence the key, so an entry that
+// matches names exactly the state looked up.  The key is the 4(n-1)-bit concatenation plus a 4-bit length
+// (memo_key_state), which fits 64 bits up to n = 16, and the value field is wide (bits >= 12).
 enum { MEMO_NONE = 0, MEMO_LANDMARK = 1, MEMO_ALL = 2, MEMO_PATH = 3 };
+
+constexpr u64 MEMO_MUL = 0x9E3779B97F4A7C15ull;   // odd (memo_slot's multiplier): a bijection mod 2^64
+
+__device__ __forceinline__ u64 path_entry(u64 key, u32 bits, u64 v) { return ((key * MEMO_MUL) << bits) | v; }
 
 __device__ __forceinline__ u64 memo_key_state(u64 w1, u64 w2, u32 n) {
     const bool sw = w2 < w1;
@@ -420,13 +430,13 @@ template <int RULE, int MODE>
 __device__ __noinline__ void memo_store_cycle(u64* T, u32 bits, u64 w1, u64 w2, u32 q4, u32 n, u32 lam) {
     const u32 lsh = memo_lam_shift<MODE>(n);
     const u32 v = MODE == MEMO_PATH ? 2u * lam : lam;
-    if (lam == 0u || (u64)v >> (64u - lsh) != 0ull) return;
+    if (lam == 0u || (u64)v >> (MODE == MEMO_PATH ? bits : 64u - lsh) != 0ull) return;
     const u32 k4m4 = 4u * (n - 1u);
     const u64 top = (u64)(n - 1u);
     for (u32 t = 0; t < lam; t++) {
         if (MODE == MEMO_PATH) {
             const u64 k = memo_key_state(w1, w2, n);
-            __stcg((unsigned long long*)T + memo_slot(k, bits), (unsigned long long)(k | ((u64)v << lsh)));
+            __stcg((unsigned long long*)T + memo_slot(k, bits), (unsigned long long)path_entry(k, bits, v));
         } else if (MODE == MEMO_ALL) memo_put(T, bits, memo_key_state(w1, w2, n), lsh, lam);
         else if ((w1 & 15ull) == top) memo_put(T, bits, memo_key(w1, w2, n), lsh, lam);
         else if ((w2 & 15ull) == top) memo_put(T, bits, memo_key(w2, w1, n), lsh, lam);
@@ -486,6 +496,7 @@ __device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __res
     u64* const memo = MEMO ? a.memo : nullptr;
     const u32 mbits = a.memo_bits, lsh = memo_lam_shift<MEMO>(n);
     const u64 kmask = lsh < 64u ? (1ull << lsh) - 1ull : ~0ull;
+    const u64 vmask = (1ull << mbits) - 1ull;   // value field of a path entry
 
     auto start_game = [&](LGame<EXTRA, MEMO>& x) {
         bool ok = CANON ? next_canon(E, a, counter, x.w1, x.w2, x.q) : next_deal(E, a, counter, dc, x.w1, x.w2, x.q);
@@ -567,9 +578,13 @@ __device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __res
             for (int i = 0; i < G; i++) {
                 LGame<EXTRA, MEMO>& x = g[i];
                 mlook += look[i] ? 1u : 0u;
-                if (look[i] && (e[i] & kmask) == key[i]) {   // (an empty slot reads 0, which is no key)
+                // (an empty slot reads 0: no key of the explicit-key memos, and a value of 0 in a path entry)
+                const bool match = MEMO == MEMO_PATH
+                    ? (e[i] & vmask) != 0ull && ((e[i] ^ path_entry(key[i], mbits, 0ull)) >> mbits) == 0ull
+                    : (e[i] & kmask) == key[i];
+                if (look[i] && match) {
                     mhit++;
-                    const u32 v = (u32)(e[i] >> lsh);
+                    const u32 v = MEMO == MEMO_PATH ? (u32)(e[i] & vmask) : (u32)(e[i] >> lsh);
                     const bool vcy = MEMO == MEMO_PATH ? (v & 1u) == 0u : true;
                     const u32 vlam = MEMO == MEMO_PATH ? v >> 1 : v;
                     if (CANON && EXTRA && a.distinct && vcy && vlam <= W && x.rounds < vlam) {
@@ -605,16 +620,21 @@ __device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __res
                     const u32 len = MEMO == MEMO_PATH && (x.mlam & 1u) ? x.rounds + (x.mlam >> 1) : x.rounds;
                     const u32 lam = (MEMO && mcy) ? mcy : x.rounds - ((x.next - W) >> 1);
                     if (MEMO == MEMO_PATH && memo != nullptr) {   // the states it missed, with its outcome
-                        const u64 vmax = 1ull << (64u - lsh);
                         if (x.ta) {
                             const u64 v = cy ? 2ull * lam : 2ull * (len - x.ta) + 1ull;
                             const u64 k = x.ka;
-                            if (v < vmax) { __stcg((unsigned long long*)memo + memo_slot(k, mbits), k | (v << lsh)); mstore++; }
+                            if (v <= vmask) {
+                                __stcg((unsigned long long*)memo + memo_slot(k, mbits), path_entry(k, mbits, v));
+                                mstore++;
+                            }
                         }
                         if (x.tb) {
                             const u64 v = cy ? 2ull * lam : 2ull * (len - x.tb) + 1ull;
                             const u64 k = x.kb;
-                            if (v < vmax) { __stcg((unsigned long long*)memo + memo_slot(k, mbits), k | (v << lsh)); mstore++; }
+                            if (v <= vmask) {
+                                __stcg((unsigned long long*)memo + memo_slot(k, mbits), path_entry(k, mbits, v));
+                                mstore++;
+                            }
                         }
                     }
                     if (cy) {

@@ -86,7 +86,8 @@ typedef struct war_tune {
                               latched records: iterations between services (rounded up to a multiple of 4) */
     int32_t variant;       /* bit 0: multiply-add turn form (else logic/shift); bit 1: outcomes latched and
                               recorded every `defer` iterations (else recorded at once); bit 2 (with
-                              bit 1, n <= 15; canonical scans only with bits 3 and 4): cycle memo, a game is decided as soon as it passes a state of
+                              bit 1; landmarks n <= 15, with bit 3 n <= 14, with bits 3 and 4 n <= 16; canonical scans only with bits 3
+                              and 4): cycle memo, a game is decided as soon as it passes a state of
                               a cycle found before in the job (`turns` then counts the turns played, fewer
                               than the reference's schedule); bit 3 (with bit 2, n <= 14): the memo holds
                               every state of the found cycles and games are looked up at their current

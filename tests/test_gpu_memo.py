@@ -53,14 +53,15 @@ def test_memo_small_table(wl, bits, variant):
 
 
 @pytest.mark.parametrize("n,lo,span", [(14, 7 * 10 ** 9, 3 * 10 ** 8), (15, 10 ** 12, 2 * 10 ** 8),
-                                       (15, 3 * 10 ** 11 + 12345, 10 ** 7), (11, 0, 39916800)])
+                                       (15, 3 * 10 ** 11 + 12345, 10 ** 7), (11, 0, 39916800),
+                                       (16, 10 ** 13, 2 * 10 ** 8), (16, 2 * 10 ** 13 + 777, 3 * 10 ** 6)])
 def test_memo_slices_vs_plain(wl, n, lo, span):
     for rule in (0, 1):
         job = wl.make_job(n, rule=rule, lo=lo, hi=lo + span, hbins=512)
         plain = wl.enumerate_plain(job)
         same(wl, wl.enumerate_job(job, memo_tune(wl)), plain)
         same(wl, wl.enumerate_job(job, memo_tune(wl, variant=15, games=1)), plain)   # all states (n <= 14)
-        same(wl, wl.enumerate_job(job, memo_tune(wl, variant=31, games=1)), plain)   # and paths
+        same(wl, wl.enumerate_job(job, memo_tune(wl, variant=31, games=1)), plain)   # and paths (n <= 16)
 
 
 def test_memo_random_ranges_with_sample(wl, oracle):
