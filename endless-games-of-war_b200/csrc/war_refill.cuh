@@ -392,7 +392,7 @@ __device__ __forceinline__ void memo_put(u64* T, u32 bits, u64 key, u32 lsh, u32
 // is looked up at its current state and needs nothing kept per turn.  Entry: the pile that is smaller as
 // a 64-bit word first (either orientation gives the same key), its cards then the other pile's as 4(n-1)
 // bits of nibbles (the last card is the one missing), its length in 4 bits, the cycle length in the top
-// 64 - 4n bits.  n <= 14.
+// 64 - 4n bits.  n <= 14.  (The path memo's entries, below, keep the key implicitly and serve n <= 16.)
 //
 // The path memo (MEMO_PATH) adds, for every decided game, the states at which it was looked up and
 // missed (the last two), with the game's outcome from there: "on a cycle of length lam" (value 2 lam) or
