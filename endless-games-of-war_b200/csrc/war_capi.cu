@@ -464,6 +464,34 @@ int war_enumerate_plain(const war_job* job, war_result* out) {
     return WAR_OK;
 }
 
+// The context's memo table for a job: 2^bits words, cleared unless the job asks to keep the table the
+// previous job of the same n, rule and key format (kind: 0 the main engine, 1 the held-out engine) left.
+static int prepare_memo(Ctx& c, const war_job* job, int bits, int kind, u64** table) {
+    cudaError_t e;
+    const size_t bytes = sizeof(u64) << bits;
+    const bool keep = (job->flags & WAR_F_MEMO_KEEP) && c.memo_bits == bits && c.memo_n == job->n &&
+                      c.memo_rule == job->rule && c.memo_kind == kind;
+    if (c.memo_bits != bits) {
+        if (c.d_memo) cudaFree(c.d_memo);
+        c.d_memo = nullptr;
+        c.memo_bits = 0;
+        if ((e = cudaMalloc(&c.d_memo, bytes)) != cudaSuccess) {
+            c.d_memo = nullptr;
+            return cuda_fail(e, "cudaMalloc cycle memo");
+        }
+        c.memo_bits = bits;
+    }
+    if (!keep && (e = cudaMemsetAsync(c.d_memo, 0, bytes, cur_stream())) != cudaSuccess) {
+        c.memo_n = -1;
+        return cuda_fail(e, "clear cycle memo");
+    }
+    c.memo_n = job->n;
+    c.memo_rule = job->rule;
+    c.memo_kind = kind;
+    *table = c.d_memo;
+    return WAR_OK;
+}
+
 int war_enumerate_held(const war_job* job, const war_tune* tune, war_result* out) {
     if (!job) return fail(WAR_EINVAL, "job is NULL");
     if (!out) return fail(WAR_EINVAL, "out is NULL");
@@ -484,12 +512,16 @@ int war_enumerate_held(const war_job* job, const war_tune* tune, war_result* out
     const int block_m = std::min(job->n, (tune && tune->block_m) ? tune->block_m : 6);
     const int W = (tune && tune->window) ? tune->window : 32;
     const int defer = (tune && tune->defer) ? tune->defer : 16;
+    const bool memo = tune && (tune->variant & 4);   // the path memo (any variant with bit 2)
+    const int memo_bits = (tune && tune->memo_bits) ? tune->memo_bits : 28;
+    if (memo && (memo_bits < 12 || memo_bits > 31)) return fail(WAR_EINVAL, "tune.memo_bits=%d (12..31)", memo_bits);
     if (threads < 64 || threads > 1024 || (threads & 31)) return fail(WAR_EINVAL, "tune.threads=%d", threads);
     if (block_m < 1 || block_m > 8) return fail(WAR_EINVAL, "tune.block_m=%d (1..8)", block_m);
     if (W < 1 || W > (1 << 16) || (W & (W - 1))) return fail(WAR_EINVAL, "tune.window=%d", W);
     if (defer < 1 || defer > 32) return fail(WAR_EINVAL, "tune.defer=%d (1..32)", defer);
-    const int maxb = held_max_blocks_per_sm(job->rule, threads, job->hbins);
-    if (maxb < 1) return fail(WAR_EINVAL, "launch shape threads=%d does not fit an SM", threads);
+    const int maxb = held_max_blocks_per_sm(job->rule, threads, job->hbins, memo);
+    if (maxb < 1) return fail(WAR_EINVAL, "launch shape threads=%d does not fit an SM%s", threads,
+                              memo ? " (at most 512 with the memo)" : "");
     const int bps = (tune && tune->blocks_per_sm) ? std::min(tune->blocks_per_sm, maxb) : maxb;
     std::lock_guard<std::mutex> lk(ctx().mu);
     Ctx& c = ctx();
@@ -506,6 +538,10 @@ int war_enumerate_held(const war_job* job, const war_tune* tune, war_result* out
     for (int i = 0; i <= 17; i++) a.fact[i] = fact(i);
     a.n = job->n; a.m = block_m; a.rule = job->rule; a.hbins = job->hbins; a.W = W; a.defer = defer;
     a.units = c.d_units;
+    if (memo) {
+        if ((st = prepare_memo(c, job, memo_bits, 1, &a.memo))) return st;
+        a.memo_bits = (u32)memo_bits;
+    }
     // each launch plays fewer than 2^32 - 2^24 games (32-bit per-lane counters)
     const u64 per_unit = fact(block_m);
     const u64 max_units = std::max<u64>(1, ((1ull << 32) - (1ull << 24)) / per_unit);
@@ -571,27 +607,8 @@ int war_enumerate(const war_job* job, const war_tune* tune, war_result* out) {
     a.seed = job->seed;
     a.thr = ((u64)job->sample_ppm << 32) / 1000000u;
     a.units = c.d_units;
-    if (t.variant & 4) {   // the cycle memo: cleared for this job unless kept from the last one of this n and rule
-        const size_t bytes = sizeof(u64) << t.memo_bits;
-        const bool keep = (job->flags & WAR_F_MEMO_KEEP) && c.memo_bits == t.memo_bits && c.memo_n == job->n &&
-                          c.memo_rule == job->rule;
-        if (c.memo_bits != t.memo_bits) {
-            if (c.d_memo) cudaFree(c.d_memo);
-            c.d_memo = nullptr;
-            c.memo_bits = 0;
-            if ((e = cudaMalloc(&c.d_memo, bytes)) != cudaSuccess) {
-                c.d_memo = nullptr;
-                return cuda_fail(e, "cudaMalloc cycle memo");
-            }
-            c.memo_bits = t.memo_bits;
-        }
-        if (!keep && (e = cudaMemsetAsync(c.d_memo, 0, bytes, cur_stream())) != cudaSuccess) {
-            c.memo_n = -1;
-            return cuda_fail(e, "clear cycle memo");
-        }
-        c.memo_n = job->n;
-        c.memo_rule = job->rule;
-        a.memo = c.d_memo;
+    if (t.variant & 4) {   // the cycle memo
+        if ((st = prepare_memo(c, job, t.memo_bits, 0, &a.memo))) return st;
         a.memo_bits = (u32)t.memo_bits;
     }
     // Each launch plays fewer than 2^32 games, so the 32-bit per-block and per-lane counters cannot wrap.

@@ -13,8 +13,9 @@
 // A unit is enumerated as (position of card n-1, order of the other cards): the others stay in deck order
 // in one word (16 nibbles at n = 17) and a unit permutes either the last j of them (card n-1 in the
 // prefix) or the last j-1 of them for each of the j positions of card n-1 in the suffix — the same set of
-// deals as the lexicographic block, so the counts are the same.
-#include "war_kernels.cuh"
+// deals as the lexicographic block, so the counts are the same.  With a table (HeldArgs.memo) the engine
+// takes the path memo of war_refill.cuh, with a key of its own state (h_key).
+#include "war_refill.cuh"
 
 namespace war {
 
@@ -141,8 +142,36 @@ __device__ __forceinline__ bool h_turn(u64& wh, u64& wo, u32& lh, u32& lo, u32& 
     return lo == 0u;
 }
 
+// Path-memo key of a held-out state (the entry format of war_refill.cuh: the key itself is not stored, the
+// slot and entry give it back).  The n-1 other cards in the order holder's then opponent's, the holder's
+// count lh and the depth p; the last card is the one missing.  At 17 cards that is 15 nibbles + 8 bits =
+// 68 bits, so there the key keeps 13 cards and the order of the last three (one of six, 3 bits): 63 bits.
+__device__ __forceinline__ u64 h_key(u64 wh, u64 wo, u32 lh, u32 p, u32 n) {
+    const u64 cat = wh | shl64(wo, 4u * lh);
+    if (n < 17u) {
+        const u32 kb = 4u * (n - 2u);
+        return (cat & ((1ull << kb) - 1ull)) | ((u64)lh << kb) | ((u64)p << (kb + 4u));
+    }
+    const u32 c0 = (u32)(cat >> 52) & 15u, c1 = (u32)(cat >> 56) & 15u, c2 = (u32)(cat >> 60) & 15u;
+    const u32 ord = 2u * ((u32)(c0 > c1) + (u32)(c0 > c2)) + (u32)(c1 > c2);
+    return (cat & ((1ull << 52) - 1ull)) | ((u64)ord << 52) | ((u64)lh << 55) | ((u64)p << 59);
+}
+
+// Walks the cycle of length lam through the given state once and stores every state (value 2 lam).
 template <int RULE>
-__global__ void __launch_bounds__(1024) held_kernel(const __grid_constant__ HeldArgs a, DevAcc* __restrict__ acc) {
+__device__ __noinline__ void h_store_cycle(u64* T, u32 bits, u64 wh, u64 wo, u32 lh, u32 lo, u32 p, u32 n, u32 lam) {
+    const u64 v = 2ull * lam;
+    if (lam == 0u || (v >> bits) != 0ull) return;
+    for (u32 t = 0; t < lam; t++) {
+        const u64 k = h_key(wh, wo, lh, p, n);
+        __stcg((unsigned long long*)T + memo_slot(k, bits), (unsigned long long)path_entry(k, bits, v));
+        h_turn<RULE>(wh, wo, lh, lo, p);
+    }
+}
+
+template <int RULE, bool MEMO>
+__global__ void __launch_bounds__(MEMO ? 512 : 1024) held_kernel(const __grid_constant__ HeldArgs a,
+                                                                DevAcc* __restrict__ acc) {
     extern __shared__ u32 sh[];
     u32* shh = sh;
     u32* she = sh + a.hbins;
@@ -160,6 +189,13 @@ __global__ void __launch_bounds__(1024) held_kernel(const __grid_constant__ Held
     u32 lh = 0, lo = 0, p = 0, tlh = 0, tp = 0, rounds = 0, next = 0;
     bool done = true, kcy = false, active = false;
     u32 cyc = 0, ndone = 0, maxfin = 0, capped = 0, turns = 0;
+    // the path memo (war_refill.cuh): lookups at every service, the game's last two misses stored with
+    // its outcome, cycles found by Brent stored whole
+    u64* const memo = MEMO ? a.memo : nullptr;
+    const u32 mbits = a.memo_bits;
+    const u64 vmask = memo ? (1ull << mbits) - 1ull : 0ull;
+    u64 ka = 0, kb = 0;
+    u32 ta = 0, tb = 0, mv = 0, mlook = 0, mhit = 0, mstore = 0;
 
     auto start_game = [&]() {
         active = false;
@@ -173,6 +209,7 @@ __global__ void __launch_bounds__(1024) held_kernel(const __grid_constant__ Held
         ndone++;
         th = wh; to = wo; tlh = lh; tp = p;
         rounds = 0; next = W; kcy = false;
+        ta = 0u; tb = 0u; mv = 0u;
         done = lo == 0u;   // n = 1 only (never here: n >= 2)
     };
 
@@ -193,16 +230,48 @@ __global__ void __launch_bounds__(1024) held_kernel(const __grid_constant__ Held
                 else { th = wh; to = wo; tlh = lh; tp = p; next = 2u * next + W; }
             }
         }
+        if (memo != nullptr) {
+            const bool look = active & !done;
+            const u64 key = h_key(wh, wo, lh, p, n);
+            const u64 e = look ? __ldcg((const unsigned long long*)memo + memo_slot(key, mbits)) : 0ull;
+            if (look) {
+                mlook++;
+                if ((e & vmask) != 0ull && ((e ^ path_entry(key, mbits, 0ull)) >> mbits) == 0ull) {
+                    mhit++;
+                    mv = (u32)(e & vmask);
+                    done = true;
+                    kcy = (mv & 1u) == 0u;
+                } else {
+                    kb = ka; tb = ta; ka = key; ta = rounds;
+                }
+            }
+        }
         if (__any_sync(WAR_FULL_MASK, done & active)) {
             if (done & active) {
                 turns += rounds;
+                const u32 mcy = (mv != 0u && (mv & 1u) == 0u) ? mv >> 1 : 0u;   // the memo's cycle length
+                const u32 len = (mv & 1u) ? rounds + (mv >> 1) : rounds;        // or the turns left
+                const u32 lam = mcy ? mcy : rounds - ((next - W) >> 1);
+                if (memo != nullptr) {
+                    if (ta) {
+                        const u64 v = kcy ? 2ull * lam : 2ull * (len - ta) + 1ull;
+                        if (v <= vmask) { __stcg((unsigned long long*)memo + memo_slot(ka, mbits), path_entry(ka, mbits, v)); mstore++; }
+                    }
+                    if (tb) {
+                        const u64 v = kcy ? 2ull * lam : 2ull * (len - tb) + 1ull;
+                        if (v <= vmask) { __stcg((unsigned long long*)memo + memo_slot(kb, mbits), path_entry(kb, mbits, v)); mstore++; }
+                    }
+                    if (kcy && mcy == 0u) {   // found by Brent: store its cycle
+                        h_store_cycle<RULE>(memo, mbits, wh, wo, lh, lo, p, n, lam);
+                        mstore += lam;
+                    }
+                }
                 if (kcy) {
-                    const u32 lam = rounds - ((next - W) >> 1);
                     cyc++;
                     if (a.hbins) atomicAdd(&shh[lam < hb1 ? lam : hb1], 1u);
                 } else {
-                    if (rounds > maxfin) maxfin = rounds;
-                    atomicAdd(&she[rounds < WAR_EBINS - 1 ? rounds : WAR_EBINS - 1], 1u);
+                    if (len > maxfin) maxfin = len;
+                    atomicAdd(&she[len < WAR_EBINS - 1 ? len : WAR_EBINS - 1], 1u);
                 }
                 start_game();
             }
@@ -212,7 +281,11 @@ __global__ void __launch_bounds__(1024) held_kernel(const __grid_constant__ Held
 
     const u64 v_cyc = warp_sum(cyc), v_done = warp_sum(ndone), v_turns = warp_sum((u64)turns), v_max = warp_max(maxfin);
     const u64 v_cap = warp_sum(capped);
+    const u64 v_l = warp_sum((u64)mlook), v_h = warp_sum((u64)mhit), v_s = warp_sum((u64)mstore);
     if ((threadIdx.x & 31) == 0) {
+        if (v_l) atomicAdd(&acc->memo_lookups, v_l);
+        if (v_h) atomicAdd(&acc->memo_hits, v_h);
+        if (v_s) atomicAdd(&acc->memo_stores, v_s);
         if (v_cyc) atomicAdd(&acc->cyc, v_cyc);
         if (v_done) atomicAdd(&acc->done, v_done);
         if (v_turns) atomicAdd(&acc->turns, v_turns);
@@ -224,19 +297,25 @@ __global__ void __launch_bounds__(1024) held_kernel(const __grid_constant__ Held
     flush_hist(she, acc->endhist, WAR_EBINS);
 }
 
+typedef void (*HeldFn)(const HeldArgs, DevAcc*);
+
+static HeldFn held_pick(int rule, bool memo) {
+    if (rule) return memo ? held_kernel<1, true> : held_kernel<1, false>;
+    return memo ? held_kernel<0, true> : held_kernel<0, false>;
+}
+
 cudaError_t launch_held(const HeldArgs& a, int threads, int blocks, DevAcc* acc, cudaStream_t st) {
     const size_t shmem = sizeof(u32) * (size_t)(a.hbins + WAR_EBINS);
-    if (a.rule) held_kernel<1><<<blocks, threads, shmem, st>>>(a, acc);
-    else held_kernel<0><<<blocks, threads, shmem, st>>>(a, acc);
+    held_pick(a.rule, a.memo != nullptr)<<<blocks, threads, shmem, st>>>(a, acc);
     note_launch();
     return cudaGetLastError();
 }
 
-int held_max_blocks_per_sm(int rule, int threads, int hbins) {
+int held_max_blocks_per_sm(int rule, int threads, int hbins, bool memo) {
+    if (memo && threads > 512) return 0;
     int nb = 0;
     const size_t shmem = sizeof(u32) * (size_t)(hbins + WAR_EBINS);
-    cudaError_t e = rule ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, held_kernel<1>, threads, shmem)
-                         : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, held_kernel<0>, threads, shmem);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, held_pick(rule, memo), threads, shmem);
     return e == cudaSuccess ? nb : 0;
 }
 

@@ -21,6 +21,7 @@ struct Ctx {
     u64* d_memo = nullptr;          // cycle memo table of the refill kernel (deals)
     int memo_bits = 0;
     int memo_n = -1, memo_rule = -1;  // job class whose cycles the memo holds
+    int memo_kind = 0;                // its key format: 0 the main engine, 1 the held-out engine
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 

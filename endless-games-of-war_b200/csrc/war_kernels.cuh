@@ -135,9 +135,11 @@ struct HeldArgs {
     u64 main_base, main_count, n_units;   // as in BatchArgs
     const Unit* units;
     int n, m, rule, hbins, W, defer;
+    u64* memo;        // path memo (2^memo_bits words, 0 = empty), or null
+    u32 memo_bits, pad;
 };
 cudaError_t launch_held(const HeldArgs& a, int threads, int blocks, DevAcc* acc, cudaStream_t st);
-int held_max_blocks_per_sm(int rule, int threads, int hbins);
+int held_max_blocks_per_sm(int rule, int threads, int hbins, bool memo);
 
 struct FloydArgs {
     u64 fact[17];

@@ -82,3 +82,53 @@ def test_refusals(wl):
         job = wl.make_job(**bad)
         with pytest.raises(warlib.WarError):
             wl.enumerate_held(job)
+
+
+def memo_held(wl, bits=24, **kw):
+    t = dict(variant=31, threads=256, memo_bits=bits)
+    t.update(kw)
+    return wl.make_tune(**t)
+
+
+@pytest.mark.parametrize("bits", [12, 24])
+def test_memo_small_n_and_slices(wl, oracle, bits):
+    """The held-out engine with the path memo (its own 63/64-bit state keys) against the oracle: every deal
+    of n <= 11, slices of n = 14..17, and a table far too small (2^12 words)."""
+    for n in range(4, 12):
+        got, want = held(wl, n, n & 1, tune=memo_held(wl, bits)), oracle_held(oracle, n, n & 1)
+        for k in FIELDS:
+            assert got[k] == want[k], (n, k)
+    rnd = random.Random(bits)
+    import math
+    for n in (14, 15, 16, 17):
+        lo = rnd.randrange(0, math.factorial(n) - 10 ** 6)
+        hi = lo + rnd.choice([777, 300001, 10 ** 6])
+        rule = rnd.randint(0, 1)
+        got, want = held(wl, n, rule, lo, hi, 256, memo_held(wl, bits)), oracle_held(oracle, n, rule, lo, hi, 256)
+        for k in FIELDS:
+            assert got[k] == want[k], (n, lo, hi, k)
+
+
+def test_memo_a13_and_long_n17_slice(wl, golden):
+    r = held(wl, 13, hbins=256, tune=memo_held(wl, 28))
+    g = golden["deals_rule0"][13]
+    assert (r["done"], r["cyc"], r["maxfin"], r["hist"]) == (g["deals"], g["cyc"], g["longest"], g["hist"])
+    lo, hi = 10 ** 14, 10 ** 14 + 2 * 10 ** 8
+    a = held(wl, 17, 0, lo, hi, 256, memo_held(wl, 26))
+    b = held(wl, 17, 0, lo, hi, 256)
+    for k in FIELDS:
+        assert a[k] == b[k], k
+
+
+def test_memo_kept_only_for_the_same_key_format(wl):
+    """A table left by the main engine (n = 16 keys) is not reused by the held-out engine, whose keys mean
+    other states, even with WAR_F_MEMO_KEEP."""
+    import warlib
+    lo, hi = 10 ** 13, 10 ** 13 + 10 ** 7
+    t_main = wl.make_tune(variant=31, games=1, threads=256, defer=8, block_m=6, memo_bits=22)
+    wl.enumerate_job(wl.make_job(16, lo=lo, hi=hi, hbins=128), t_main)
+    job = wl.make_job(16, flags=warlib.F_MEMO_KEEP, lo=lo, hi=hi, hbins=128)
+    a = wl.to_dict(wl.enumerate_held(job, memo_held(wl, 22)))
+    b = held(wl, 16, 0, lo, hi, 128)
+    for k in FIELDS:
+        assert a[k] == b[k], k
