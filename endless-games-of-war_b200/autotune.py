@@ -62,7 +62,7 @@ def default_tune(n, mode, rule, flags):
     if mode != warlib.DEALS or n < 4:
         return None
     bits = {4: 12, 5: 12, 6: 14, 7: 16, 8: 18, 9: 20, 10: 22, 11: 24, 12: 27}.get(n, 30)
-    variant = 31   # the path memo (n <= 16)
+    variant = 31 if n <= 16 else 3   # the path memo up to 16 cards (it loses on 17-card slices)
     return {"block_m": min(6, n), "blocks_per_sm": 0, "defer": 8, "games": 1, "threads": 256, "window": 32,
             "variant": variant, "memo_bits": bits}
 
