@@ -60,8 +60,9 @@ static ServeFn serve_pick(bool canon, bool shape, bool extra) {
 }
 
 // Launch shapes of the serving kernel: one game per thread, 256-thread blocks, the multiply-add turn form;
-// latched records with the path memo where it applies (memo = 1: n <= 16 and a table), latched records
-// without it otherwise, and the immediate-record loop for the loop-shape test.
+// latched records with the path memo where it applies (memo = 1: n <= 14 and a table), with the landmark
+// memo for deals of n = 15 (memo = 2), latched records without a memo otherwise, and the immediate-record
+// loop for the loop-shape test.
 struct Variant {
     int canon, rule, shape, extra, memo;
     bool operator<(const Variant& o) const {
@@ -73,9 +74,11 @@ struct Variant {
     ServeFn fn() const {
         const bool c = canon != 0;
         if (rule) return shape ? serve_pick<1, 1, 1>(c, true, extra)
-                             : memo ? serve_pick<1, 1, 31>(c, false, extra) : serve_pick<1, 1, 3>(c, false, extra);
+                         : memo == 1 ? serve_pick<1, 1, 31>(c, false, extra)
+                         : memo == 2 ? serve_pick<1, 1, 7>(c, false, extra) : serve_pick<1, 1, 3>(c, false, extra);
         return shape ? serve_pick<0, 1, 1>(c, true, extra)
-                     : memo ? serve_pick<0, 1, 31>(c, false, extra) : serve_pick<0, 1, 3>(c, false, extra);
+                     : memo == 1 ? serve_pick<0, 1, 31>(c, false, extra)
+                     : memo == 2 ? serve_pick<0, 1, 7>(c, false, extra) : serve_pick<0, 1, 3>(c, false, extra);
     }
 };
 
@@ -164,7 +167,8 @@ void set_args(war_server* s, SJob& J) {
     J.var.shape = a.blk ? 1 : 0;
     J.var.extra = (a.distinct || a.sample) ? 1 : 0;
     J.var.memo = 0;
-    if (!a.blk && job.n >= 4 && job.n <= 16 && s->cfg.memo_bits >= 0) {
+    const bool landmarks = !canon && job.n == 15;   // the landmark memo serves n = 15 deals
+    if (!a.blk && job.n >= 4 && (job.n <= 14 || landmarks) && s->cfg.memo_bits >= 0) {
         // the class's table: 2^bits words, grown with n (about a thousandth of the class's rank space)
         const std::pair<int, int> cls(job.n, job.rule);
         auto it = s->memos.find(cls);
@@ -183,7 +187,7 @@ void set_args(war_server* s, SJob& J) {
         if (it->second.first) {
             a.memo = it->second.first;
             a.memo_bits = (u32)it->second.second;
-            J.var.memo = 1;
+            J.var.memo = landmarks ? 2 : 1;
         }
     }
 }
