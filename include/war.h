@@ -84,17 +84,17 @@ typedef struct war_tune {
     int32_t window;        /* Brent first tortoise window (power of two); 1 = the reference's schedule */
     int32_t defer;         /* immediate records: lanes that wait, decided, before the warp refills them (1..32);
                               latched records: iterations between services (rounded up to a multiple of 4) */
-    int32_t variant;       /* bit 0: multiply-add turn form (else logic/shift); bit 1: outcomes latched and
-                              recorded every `defer` iterations (else recorded at once); bit 2 (with
-                              bit 1; landmarks n <= 15, with bit 3 n <= 14, with bits 3 and 4 n <= 16; canonical scans only with bits 3
-                              and 4): cycle memo, a game is decided as soon as it passes a state of
-                              a cycle found before in the job (`turns` then counts the turns played, fewer
-                              than the reference's schedule); bit 3 (with bit 2, n <= 14): the memo holds
-                              every state of the found cycles and games are looked up at their current
-                              state (else cycle landmarks, kept per turn); bit 4 (with bits 2 and 3): the
-                              memo also holds states on the paths of decided games with their outcome
-                              (cycle length or turns left), so games that merge into an earlier game's path
-                              are decided there; same results otherwise */
+    int32_t variant;       /* bit 0: multiply-add turn form (else logic/shift).
+                              bit 1: outcomes latched and recorded every `defer` iterations (else at once).
+                              bit 2 (needs bit 1 and n >= 4): the cycle memo, a table of facts "from this
+                              state the game cycles with length L / ends after r turns" filled by the job's
+                              own games; a game is decided at the first state it finds there (`turns` then
+                              counts the turns played, fewer than the reference's schedule).  Alone: the
+                              memo holds cycle landmarks kept per turn (n <= 15).  With bit 3: every state
+                              of each found cycle, games looked up at their current state (n <= 14).  With
+                              bits 3 and 4 (the "path memo"): also the states where decided games missed,
+                              with their outcome (n <= 16; canonical scans take only this form).
+                              Every form gives the same results; out-of-range forms fall back to none. */
     int32_t memo_bits;     /* cycle memo: log2 of its 8-byte slots (12..31); 0 = 24 (128 MiB) */
 } war_tune;
 
