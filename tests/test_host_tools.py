@@ -1,0 +1,60 @@
+"""Host-side helpers that need no GPU: the serving workload generator and its statistics, and the
+autotuner's defaults and legality rules."""
+import math
+
+
+def test_poisson_stream_is_seeded_and_in_range():
+    import serve
+    import warlib
+    a = serve.poisson_stream(3000, rate=100.0, seed=11)
+    b = serve.poisson_stream(3000, rate=100.0, seed=11)
+    assert [(t, j.n, j.mode, j.lo, j.hi) for t, j in a] == [(t, j.n, j.mode, j.lo, j.hi) for t, j in b]
+    times = [t for t, _ in a]
+    assert times == sorted(times) and times[0] > 0
+    assert abs(len(a) / times[-1] - 100.0) < 10.0                    # Poisson arrivals at the given rate
+    deals = 0
+    for _, j in a:
+        assert j.n in (9, 10, 11, 13, 14, 15)
+        total = warlib.space_size(j.n, j.mode)
+        assert 0 <= j.lo < j.hi <= total
+        assert j.hi - j.lo == min(total, j.hi - j.lo)
+        assert j.hi - j.lo <= 10 ** 9 and (j.hi - j.lo >= 10 ** 4 or j.hi - j.lo == total)
+        deals += j.mode == warlib.DEALS
+    assert 0.65 < deals / len(a) < 0.75                                # 70% deals
+
+
+def test_percentile():
+    import serve
+    xs = list(range(1, 101))
+    assert serve.percentile(xs, 50) == 50 and serve.percentile(xs, 99) == 99 and serve.percentile(xs, 100) == 100
+    assert serve.percentile([], 50) is None
+
+
+def test_default_tunes():
+    import autotune
+    import warlib
+    assert autotune.default_tune(13, warlib.CANON, 0, 0) is None
+    assert autotune.default_tune(3, warlib.DEALS, 0, 0) is None
+    t13, t17 = autotune.default_tune(13, warlib.DEALS, 0, 0), autotune.default_tune(17, warlib.DEALS, 0, 0)
+    assert t13["variant"] == 31 and t17["variant"] == 3
+    bits = [autotune.default_tune(n, warlib.DEALS, 0, 0)["memo_bits"] for n in range(4, 17)]
+    assert bits == sorted(bits) and 12 <= bits[0] and bits[-1] <= 31
+    assert all(autotune.default_tune(n, warlib.DEALS, 0, 0)["block_m"] <= n for n in range(4, 18))
+
+
+def test_autotune_legality():
+    import autotune
+    import warlib
+    base = dict(autotune.DEFAULT)
+    assert autotune._legal(13, warlib.DEALS, 0, base)
+    assert not autotune._legal(13, warlib.DEALS, 0, dict(base, games=2, threads=1024))
+    assert not autotune._legal(4, warlib.DEALS, 0, dict(base, block_m=5))
+    assert not autotune._legal(14, warlib.CANON, warlib.F_DISTINCT, dict(base, window=32))   # on-cycle test needs W >= lam
+    assert autotune._legal(14, warlib.CANON, warlib.F_DISTINCT, dict(base, window=128))
+
+
+def test_space_sizes():
+    import warlib
+    assert warlib.space_size(13) == math.factorial(13)
+    assert warlib.space_size(14, warlib.CANON) == math.factorial(13) * 13
+    assert warlib.space_size(1, warlib.CANON) == 0
