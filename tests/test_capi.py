@@ -111,3 +111,36 @@ def test_plan_full_space_is_main_units():
     assert (mb, mc, extra) == (0, fact(13) // fact(6), [])
     mb, mc, extra = warlib.plan(warlib.make_job(14, warlib.CANON), 5)
     assert (mb, mc, extra) == (0, fact(13) // fact(5), [])
+
+
+C_CALLER = r"""
+#include "war.h"
+#include <stdio.h>
+#include <stdlib.h>
+int main(void) {
+    war_job job = { .n = 11, .mode = WAR_DEALS, .hbins = 64, .lo = 0, .hi = 39916800ull };
+    war_tune t = { .threads = 256, .games = 1, .block_m = 6, .window = 32, .defer = 8, .variant = 31, .memo_bits = 20 };
+    war_result* r = (war_result*)malloc(sizeof *r);
+    int st = war_enumerate(&job, &t, r);
+    if (st != WAR_OK) { char e[256]; war_last_error(e, sizeof e); printf("status %d: %s\n", st, e); return 0; }
+    printf("a(11)=%llu longest=%llu\n", (unsigned long long)r->cyc, (unsigned long long)r->maxfin);
+    return 0;
+}
+"""
+
+
+def test_header_is_plain_c_and_links(tmp_path):
+    """include/war.h compiles as strict C99 and a C program links against libwar.so and runs: on a machine
+    without a GPU it gets WAR_ENODEV and a message, with one it prints a(11)."""
+    import os
+    import subprocess
+    import warlib
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = tmp_path / "caller.c"
+    src.write_text(C_CALLER)
+    exe = tmp_path / "caller"
+    libdir = os.path.dirname(warlib.LIB_PATH)
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", "-I", os.path.join(root, "include"),
+                    str(src), "-L", libdir, "-lwar", "-Wl,-rpath," + libdir, "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120).stdout
+    assert out.startswith("status -8:") or out.startswith("a(11)=28223770 longest=41"), out
