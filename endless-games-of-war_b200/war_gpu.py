@@ -1,4 +1,5 @@
-"""Count the deals of single-suit War that never end, on a B200 (n <= 16).
+"""Count the deals of single-suit War that never end, on a B200 (n <= 16; deals of 17 cards go to the
+held-out-card engine, see war17.py).
 
 Drop-in for the reference's gpu/war_gpu.py: the same command line, the same run() signature and return
 tuple, the same output lines and the same <out>.progress file (gpu/war_gpu.py:272-398).  The work runs
