@@ -8,14 +8,19 @@ at a time, over
     threads        block size                                            (128..1024)
     blocks_per_sm  resident blocks (0 = as many as fit)
     window         Brent's first tortoise window                         (8..128)
-    defer          lanes that wait, decided, before the warp refills     (1..8)
+    defer          immediate records: lanes that wait before the warp refills; latched records: turns
+                   between services                                      (1..32)
     variant        bit 0: multiply-add turn form; bit 1: latched records serviced every `defer` iterations;
                    bit 2: cycle memo (deals); bit 3: the memo holds every cycle state; bit 4: and paths
+    memo_bits      log2 of the memo table's 8-byte words                 (26..30)
 Every configuration must return exactly the same counts as the first one; a mismatch raises.  The best
 configuration is stored in tune_cache.json next to this file, keyed by GPU name, n, mode, rule and flags.
 
-    python autotune.py 13                 deals, n = 13
-    python autotune.py 14 --canon --distinct
+The cycle memo is cleared per job and pays only once it has warmed up, so a short slice favours the
+variants without it: tune memo configurations on the whole space (--full) or on a long slice.
+
+    python autotune.py 13                         deals, n = 13 (its whole space takes well under a second)
+    python autotune.py 14 --canon --distinct --full
 """
 import argparse
 import json
@@ -36,7 +41,7 @@ SPACE = {
     "window": [8, 16, 32, 64, 128],
     "defer": [1, 2, 4, 6, 8, 12, 16, 24, 32],
     "variant": [0, 1, 2, 3, 6, 7, 14, 15, 30, 31],
-    "memo_bits": [24, 25, 26, 27, 28],
+    "memo_bits": [26, 28, 29, 30],
 }
 DEFAULT = {"block_m": 5, "games": 2, "threads": 512, "blocks_per_sm": 0, "window": 32, "defer": 8, "variant": 1,
            "memo_bits": 24}
@@ -172,10 +177,12 @@ def main():
     ap.add_argument("--distinct", action="store_true")
     ap.add_argument("--shape", action="store_true")
     ap.add_argument("--slice-s", type=float, default=0.4)
+    ap.add_argument("--full", action="store_true", help="time every configuration on the whole space")
     ap.add_argument("--passes", type=int, default=2)
     a = ap.parse_args()
     flags = (warlib.F_DISTINCT if a.distinct else 0) | (warlib.F_SHAPE if a.shape else 0)
-    e = autotune(a.n, warlib.CANON if a.canon else warlib.DEALS, a.rule, flags, a.slice_s, a.passes)
+    e = autotune(a.n, warlib.CANON if a.canon else warlib.DEALS, a.rule, flags, 1e9 if a.full else a.slice_s,
+                 a.passes)
     print(json.dumps(e))
 
 
