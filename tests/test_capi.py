@@ -144,3 +144,17 @@ def test_header_is_plain_c_and_links(tmp_path):
                     str(src), "-L", libdir, "-lwar", "-Wl,-rpath," + libdir, "-o", str(exe)], check=True)
     out = subprocess.run([str(exe)], capture_output=True, text=True, timeout=120).stdout
     assert out.startswith("status -8:") or out.startswith("a(11)=28223770 longest=41"), out
+
+
+def test_held_engine_argument_errors():
+    """war_enumerate_held validates before touching the device: bad jobs fail with WAR_EINVAL on any
+    machine, an empty range succeeds without one."""
+    import warlib
+    for bad in (dict(n=1), dict(n=18, hi=1), dict(n=9, mode=warlib.CANON), dict(n=9, rule=2),
+                dict(n=9, flags=warlib.F_SAMPLE), dict(n=9, flags=warlib.F_HALF), dict(n=9, hbins=5000),
+                dict(n=17, hi=math.factorial(17) + 1), dict(n=9, lo=5, hi=4)):
+        with pytest.raises(warlib.WarError) as e:
+            warlib.enumerate_held(warlib.make_job(**bad))
+        assert e.value.status == -1, bad
+    r = warlib.enumerate_held(warlib.make_job(17, lo=123, hi=123, hbins=16))
+    assert (r.done, r.cyc, r.hbins) == (0, 0, 16)
