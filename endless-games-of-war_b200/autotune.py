@@ -61,13 +61,16 @@ def load_cache():
 
 
 def default_tune(n, mode, rule, flags):
-    """The tune for a job class with no stored entry: for deals, the path memo with a table that grows
-    with n (the n = 13 measurements: 6! work units, services every 8 turns, one game per lane); for
-    canonical scans, None (the library's defaults)."""
-    if mode != warlib.DEALS or n < 4:
+    """The tune for a job class with no stored entry: the path memo with a table that grows with n (the
+    n = 13 deal and n = 14 canonical measurements: 6! (deals) or 5! x splits (canonical) work units,
+    services every 8 (deals) or 16 (canonical) turns, one game per lane); none below 4 cards."""
+    if n < 4:
         return None
     bits = {4: 12, 5: 12, 6: 14, 7: 16, 8: 18, 9: 20, 10: 22, 11: 24, 12: 27}.get(n, 30)
     variant = 31 if n <= 16 else 3   # the path memo up to 16 cards (it loses on 17-card slices)
+    if mode == warlib.CANON:
+        return {"block_m": min(5, n - 1), "blocks_per_sm": 0, "defer": 16, "games": 1, "threads": 512,
+                "window": 128, "variant": variant, "memo_bits": bits}
     return {"block_m": min(6, n), "blocks_per_sm": 0, "defer": 8, "games": 1, "threads": 256, "window": 32,
             "variant": variant, "memo_bits": bits}
 

@@ -465,7 +465,8 @@ int war_enumerate_plain(const war_job* job, war_result* out) {
 }
 
 // The context's memo table for a job: 2^bits words, cleared unless the job asks to keep the table the
-// previous job of the same n, rule and key format (kind: 0 the main engine, 1 the held-out engine) left.
+// previous job of the same n, rule and key format (kind: 0 the main engine, 1 the held-out engine, 2 the
+// main engine's shape-carrying values) left.
 static int prepare_memo(Ctx& c, const war_job* job, int bits, int kind, u64** table) {
     cudaError_t e;
     const size_t bytes = sizeof(u64) << bits;
@@ -608,7 +609,9 @@ int war_enumerate(const war_job* job, const war_tune* tune, war_result* out) {
     a.thr = ((u64)job->sample_ppm << 32) / 1000000u;
     a.units = c.d_units;
     if (t.variant & 4) {   // the cycle memo
-        if ((st = prepare_memo(c, job, t.memo_bits, 0, &a.memo))) return st;
+        // kind 2: the shape-carrying values of a canonical scan with the loop-shape test
+        const int kind = (job->mode == WAR_CANON && (job->flags & WAR_F_SHAPE)) ? 2 : 0;
+        if ((st = prepare_memo(c, job, t.memo_bits, kind, &a.memo))) return st;
         a.memo_bits = (u32)t.memo_bits;
     }
     // Each launch plays fewer than 2^32 games, so the 32-bit per-block and per-lane counters cannot wrap.

@@ -427,9 +427,10 @@ __device__ __forceinline__ u32 memo_lam_shift(u32 n) { return MODE >= MEMO_ALL ?
 // Walks the cycle of length lam through the state (w1, w2, q4 = 4*len1) once and stores its landmarks
 // (MEMO_LANDMARK) or all its states (MEMO_ALL, MEMO_PATH).
 template <int RULE, int MODE>
-__device__ __noinline__ void memo_store_cycle(u64* T, u32 bits, u64 w1, u64 w2, u32 q4, u32 n, u32 lam) {
+__device__ __noinline__ void memo_store_cycle(u64* T, u32 bits, u64 w1, u64 w2, u32 q4, u32 n, u32 lam,
+                                              u32 pv = 0u) {
     const u32 lsh = memo_lam_shift<MODE>(n);
-    const u32 v = MODE == MEMO_PATH ? 2u * lam : lam;
+    const u32 v = MODE == MEMO_PATH ? (pv ? pv : 2u * lam) : lam;   // pv: the path value, if not 2 lam
     if (lam == 0u || (u64)v >> (MODE == MEMO_PATH ? bits : 64u - lsh) != 0ull) return;
     const u32 k4m4 = 4u * (n - 1u);
     const u64 top = (u64)(n - 1u);
@@ -461,13 +462,18 @@ struct LGame {
     u32 mlam;           // MEMO: the memo's value for this game (0: decided by Brent or by its end)
     u64 ka, kb;         // MEMO_PATH: the keys of the last two states looked up and missed,
     u32 ta, tb;         // at these turns (0: none)
-    u32 pend;           // canonical distinct scan: the memo's cycle length, held until turn pend (0: none)
+    u32 pend;           // canonical distinct scan: a memo value held until turn lam of its cycle (0: none)
 };
 
 // With MEMO_LANDMARK, each turn also keeps the state before it when card n-1 is on top (a landmark), and
 // every service looks the kept landmark of each undecided game up in the memo; with MEMO_ALL every
 // service looks up each undecided game's current state.  A game decided by Brent stores its cycle.
-template <int RULE, int G, bool CANON, bool EXTRA, int TV, int MEMO>
+//
+// SHAPE (canonical scans with the loop-shape test, path memo only): the Theorem-3 shape is a property of
+// the cycle, so it travels in the memo with the cycle length — a cycle outcome is 8 lam + 2 code (code 0
+// of the shape, 1 not, 2 loop too long to check) instead of 2 lam — and a cycle found by Brent is checked
+// once with loop_shape_walk from its detection state, which lies on the loop.
+template <int RULE, int G, bool CANON, bool EXTRA, int TV, int MEMO, bool SHAPE = false>
 __device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __restrict__ acc, u64* __restrict__ counter,
                                                u32* sh) {
     u32* shh = sh;
@@ -491,6 +497,7 @@ __device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __res
     LGame<EXTRA, MEMO> g[G];
     u32 cyc = 0, done = 0, maxfin = 0, capped = 0, turns = 0;
     u32 sc = 0, scy = 0, slam = 0, slen = 0, smax = 0, oncyc = 0, dmin = 0;
+    u32 nonstd = 0, unchk = 0;             // SHAPE
     u32 mlook = 0, mhit = 0, mstore = 0;   // memo traffic
     const u32 nm1 = n - 1u;
     u64* const memo = MEMO ? a.memo : nullptr;
@@ -586,18 +593,18 @@ __device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __res
                     mhit++;
                     const u32 v = MEMO == MEMO_PATH ? (u32)(e[i] & vmask) : (u32)(e[i] >> lsh);
                     const bool vcy = MEMO == MEMO_PATH ? (v & 1u) == 0u : true;
-                    const u32 vlam = MEMO == MEMO_PATH ? v >> 1 : v;
+                    const u32 vlam = MEMO == MEMO_PATH ? v >> (SHAPE ? 3 : 1) : v;
                     if (CANON && EXTRA && a.distinct && vcy && vlam <= W && x.rounds < vlam) {
                         // Whether the start lies on its cycle shows at turn vlam: Brent's first window
                         // compares every state up to W >= vlam with the start.  Play on until then.
-                        x.pend = vlam;
+                        x.pend = v;
                     } else {
                         x.done = true; x.kcy = vcy; x.mlam = v;
                     }
-                } else if (CANON && EXTRA && x.pend != 0u && !x.done && x.rounds >= x.pend) {
-                    // turn pend passed without the start coming back: on the cycle of length pend, not
-                    // through the start
-                    x.done = true; x.kcy = true; x.mlam = MEMO == MEMO_PATH ? 2u * x.pend : x.pend;
+                } else if (CANON && EXTRA && x.pend != 0u && !x.done &&
+                           x.rounds >= (MEMO == MEMO_PATH ? x.pend >> (SHAPE ? 3 : 1) : x.pend)) {
+                    // turn lam passed without the start coming back: on the cycle, not through the start
+                    x.done = true; x.kcy = true; x.mlam = x.pend;
                 } else if (MEMO == MEMO_PATH && look[i]) {
                     x.kb = x.ka; x.tb = x.ta;
                     x.ka = key[i]; x.ta = x.rounds;
@@ -616,12 +623,21 @@ __device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __res
                     const bool cy = x.kcy;
                     turns += x.rounds;
                     // the memo's cycle length, or (path memo) the turns left after the memoised state
-                    const u32 mcy = MEMO == MEMO_PATH ? (x.mlam & 1u ? 0u : x.mlam >> 1) : x.mlam;
+                    const u32 mcy = MEMO == MEMO_PATH ? (x.mlam & 1u ? 0u : x.mlam >> (SHAPE ? 3 : 1)) : x.mlam;
                     const u32 len = MEMO == MEMO_PATH && (x.mlam & 1u) ? x.rounds + (x.mlam >> 1) : x.rounds;
                     const u32 lam = (MEMO && mcy) ? mcy : x.rounds - ((x.next - W) >> 1);
+                    // SHAPE: the loop's shape code, from the memo or checked now on the loop
+                    u32 code = 0u;
+                    if (SHAPE && cy) {
+                        code = mcy ? (x.mlam >> 1) & 3u
+                                   : (u32)loop_shape_walk<RULE>(x.w1, x.w2, TV ? x.q + qshift : x.q, k4m4, lam, (u32)a.blk);
+                        if (code == 1u) nonstd++;
+                        if (code == 2u) unchk++;
+                    }
+                    const u64 vcyc = SHAPE ? 8ull * lam + 2ull * code : 2ull * lam;   // the cycle outcome
                     if (MEMO == MEMO_PATH && memo != nullptr) {   // the states it missed, with its outcome
                         if (x.ta) {
-                            const u64 v = cy ? 2ull * lam : 2ull * (len - x.ta) + 1ull;
+                            const u64 v = cy ? vcyc : 2ull * (len - x.ta) + 1ull;
                             const u64 k = x.ka;
                             if (v <= vmask) {
                                 __stcg((unsigned long long*)memo + memo_slot(k, mbits), path_entry(k, mbits, v));
@@ -629,7 +645,7 @@ __device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __res
                             }
                         }
                         if (x.tb) {
-                            const u64 v = cy ? 2ull * lam : 2ull * (len - x.tb) + 1ull;
+                            const u64 v = cy ? vcyc : 2ull * (len - x.tb) + 1ull;
                             const u64 k = x.kb;
                             if (v <= vmask) {
                                 __stcg((unsigned long long*)memo + memo_slot(k, mbits), path_entry(k, mbits, v));
@@ -640,7 +656,8 @@ __device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __res
                     if (cy) {
                         cyc++;
                         if (MEMO && memo != nullptr && mcy == 0u) {   // found by Brent: store its cycle
-                            memo_store_cycle<RULE, MEMO>(memo, mbits, x.w1, x.w2, TV ? x.q + qshift : x.q, n, lam);
+                            memo_store_cycle<RULE, MEMO>(memo, mbits, x.w1, x.w2, TV ? x.q + qshift : x.q, n, lam,
+                                                         SHAPE ? (u32)vcyc : 0u);
                             mstore += lam;
                         }
                         if (a.hbins) atomicAdd(&shh[lam < hb1 ? lam : hb1], 1u);
@@ -681,6 +698,13 @@ __device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __res
         }
     }
 
+    if (SHAPE) {
+        u64 v_ns = warp_sum((u64)nonstd), v_un = warp_sum((u64)unchk);
+        if ((threadIdx.x & 31) == 0) {
+            if (v_ns) atomicAdd(&acc->shape_nonstd, v_ns);
+            if (v_un) atomicAdd(&acc->shape_unchecked, v_un);
+        }
+    }
     if (MEMO) {
         u64 v_l = warp_sum((u64)mlook), v_h = warp_sum((u64)mhit), v_s = warp_sum((u64)mstore);
         if ((threadIdx.x & 31) == 0) {
@@ -721,7 +745,9 @@ __device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __res
 template <int RULE, int G, bool CANON, bool SHAPE, bool EXTRA, int V>
 __device__ __forceinline__ void refill_dispatch(const BatchArgs& a, DevAcc* __restrict__ acc, u64* __restrict__ counter,
                                                 u32* sh) {
-    if constexpr (SHAPE || (V & 2) == 0) refill_body<RULE, G, CANON, SHAPE, EXTRA, V & 1>(a, acc, counter, sh);
+    if constexpr (SHAPE && CANON && (V & 30) == 30)   // the loop-shape test with the path memo
+        refill_latched<RULE, G, CANON, EXTRA, V & 1, MEMO_PATH, true>(a, acc, counter, sh);
+    else if constexpr (SHAPE || (V & 2) == 0) refill_body<RULE, G, CANON, SHAPE, EXTRA, V & 1>(a, acc, counter, sh);
     else if constexpr ((V & 4) == 0 || (CANON && (V & 8) == 0)) refill_latched<RULE, G, CANON, EXTRA, V & 1, MEMO_NONE>(a, acc, counter, sh);
     else if constexpr ((V & 24) == 24) refill_latched<RULE, G, CANON, EXTRA, V & 1, MEMO_PATH>(a, acc, counter, sh);
     else if constexpr ((V & 8) != 0) refill_latched<RULE, G, CANON, EXTRA, V & 1, MEMO_ALL>(a, acc, counter, sh);

@@ -150,3 +150,40 @@ def test_memo_canon_n13_n14_full(wl, golden):
         plain = wl.to_dict(wl.enumerate_job(job))   # the same scan without the memo
         for k in FIELDS + ("hist", "dhist", "endhist"):
             assert r[k] == plain[k], (n, k)
+
+
+@pytest.mark.parametrize("variant", [30, 31])
+def test_memo_canon_shape_small_vs_oracle(wl, oracle, variant):
+    """The loop-shape test (--shape) with the path memo: the shape code travels with the cycle length."""
+    for n in (5, 7, 8, 9, 10, 11):
+        for rule in (0, 1):
+            F = wl.F_DISTINCT | wl.F_SHAPE
+            job = wl.make_job(n, wl.CANON, rule=rule, flags=F, hbins=256, dbins=256)
+            want = oracle.to_dict(oracle.enumerate_job(oracle.make_job(n, 1, rule, F, 0, job.hi, 256, 256)))
+            got = wl.to_dict(wl.enumerate_job(job, memo_tune(wl, variant=variant, window=128, memo_bits=20)))
+            for k in FIELDS + ("hist", "dhist", "endhist"):
+                assert got[k] == want[k], (n, rule, k)
+    rnd = random.Random(5)
+    for n in (10, 11):
+        total = wl.space_size(n, wl.CANON)
+        lo = rnd.randrange(0, total - 400000)
+        job = wl.make_job(n, wl.CANON, flags=wl.F_SHAPE, lo=lo, hi=lo + 400000, hbins=128)
+        want = oracle.to_dict(oracle.enumerate_job(oracle.make_job(n, 1, 0, wl.F_SHAPE, lo, lo + 400000, 128, 0)))
+        got = wl.to_dict(wl.enumerate_job(job, memo_tune(wl, variant=variant, window=128, memo_bits=16)))
+        for k in FIELDS + ("hist", "endhist"):
+            assert got[k] == want[k], (n, lo, k)
+
+
+def test_memo_canon_shape_n13_n14_full(wl, golden):
+    """`war_gpu.py 13/14 --canon --distinct --shape` with the path memo against the recorded values (data/
+    checks.txt:180-182, data/long_runs.txt:20-23), the shape counts included."""
+    for n in (13, 14):
+        job = wl.make_job(n, wl.CANON, flags=wl.F_DISTINCT | wl.F_SHAPE, hbins=256, dbins=4096)
+        r = wl.to_dict(wl.enumerate_job(job, memo_tune(wl, variant=31, games=1, threads=512, block_m=5, window=128,
+                                                       defer=16, memo_bits=28)))
+        g = golden["canon_rule0"][n]
+        assert (r["done"], r["cyc"], r["maxfin"], r["dhist"]) == (g["positions"], g["cycling"], g["longest"], g["dhist"])
+        assert r["distinct_min"] == g["distinct"]
+        assert (r["shape_nonstd"], r["shape_unchecked"]) == (g["shape_nonstd"], g["shape_unchecked"])
+        if "hist" in g:
+            assert r["hist"] == g["hist"]

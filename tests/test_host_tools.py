@@ -33,7 +33,8 @@ def test_percentile():
 def test_default_tunes():
     import autotune
     import warlib
-    assert autotune.default_tune(13, warlib.CANON, 0, 0) is None
+    c14 = autotune.default_tune(14, warlib.CANON, 0, warlib.F_DISTINCT | warlib.F_SHAPE)
+    assert c14["variant"] == 31 and c14["window"] >= 128            # the free on-cycle test needs W >= lam
     assert autotune.default_tune(3, warlib.DEALS, 0, 0) is None
     t13, t17 = autotune.default_tune(13, warlib.DEALS, 0, 0), autotune.default_tune(17, warlib.DEALS, 0, 0)
     assert t13["variant"] == 31 and t17["variant"] == 3
