@@ -520,7 +520,8 @@ int war_enumerate_held(const war_job* job, const war_tune* tune, war_result* out
     if (block_m < 1 || block_m > 8) return fail(WAR_EINVAL, "tune.block_m=%d (1..8)", block_m);
     if (W < 1 || W > (1 << 16) || (W & (W - 1))) return fail(WAR_EINVAL, "tune.window=%d", W);
     if (defer < 1 || defer > 32) return fail(WAR_EINVAL, "tune.defer=%d (1..32)", defer);
-    const int maxb = held_max_blocks_per_sm(job->rule, threads, job->hbins, memo);
+    const bool fma = tune && (tune->variant & 1);   // the multiply-add, branch-free turn
+    const int maxb = held_max_blocks_per_sm(job->rule, threads, job->hbins, memo, fma);
     if (maxb < 1) return fail(WAR_EINVAL, "launch shape threads=%d does not fit an SM%s", threads,
                               memo ? " (at most 512 with the memo)" : "");
     const int bps = (tune && tune->blocks_per_sm) ? std::min(tune->blocks_per_sm, maxb) : maxb;
@@ -539,6 +540,8 @@ int war_enumerate_held(const war_job* job, const war_tune* tune, war_result* out
     for (int i = 0; i <= 17; i++) a.fact[i] = fact(i);
     a.n = job->n; a.m = block_m; a.rule = job->rule; a.hbins = job->hbins; a.W = W; a.defer = defer;
     a.units = c.d_units;
+    a.fma = fma ? 1 : 0;
+    a.tk.k16 = 16u; a.tk.km16 = (u32)-16; a.tk.k2p28 = 1u << 28; a.tk.k4 = 4u; a.tk.one = 1u;
     if (memo) {
         if ((st = prepare_memo(c, job, memo_bits, 1, &a.memo))) return st;
         a.memo_bits = (u32)memo_bits;

@@ -142,6 +142,39 @@ __device__ __forceinline__ bool h_turn(u64& wh, u64& wo, u32& lh, u32& lo, u32& 
     return lo == 0u;
 }
 
+// The same turn without a branch and with the card arithmetic on the multiply-add pipe, the way
+// war_turn_fma does it for the main engine: both tops are popped (funnel shift, multiply-high, card =
+// lo - 16 lo'), the holder's pop is undone by a select when it plays card n-1, and the one or two cards
+// that go under the winner's pile are added to its word by a multiply-add with a 0/1 weight (the nibbles
+// above a pile are zero, so adding is placing).  K: the constants of war_turn_fma.
+template <int RULE>
+__device__ __forceinline__ bool h_turn_fma(u64& wh, u64& wo, u32& lh, u32& lo, u32& p, const TurnK& K) {
+    const u32 ol = (u32)wo, oh = (u32)(wo >> 32), hl = (u32)wh, hh = (u32)(wh >> 32);
+    const u32 nol = __funnelshift_r(ol, oh, 4), noh = __umulhi(oh, K.k2p28);
+    const u32 nhl = __funnelshift_r(hl, hh, 4), nhh = __umulhi(hh, K.k2p28);
+    const u32 c = ol + nol * K.km16;                   // the opponent's top card
+    const u32 h = hl + nhl * K.km16;                   // the holder's top other card (played when p != 0)
+    const bool z = p == 0u;                            // the holder plays card n-1
+    const bool hw = z | (h > c);                       // the holder wins the turn
+    const u32 hi = max(h, c), lw = min(h, c);
+    const u32 pair = RULE ? lw + hi * K.k16 : hi + lw * K.k16;
+    const u32 t = z ? c : pair;                        // what goes under the winner's pile
+    const u32 lh1 = z ? lh : lh - 1u, lo1 = lo - 1u;   // counts after the pops
+    const u32 pos = 4u * (hw ? lh1 : lo1);
+    const u64 x = shl64((u64)t, pos);
+    const u32 xl = (u32)x, xh = (u32)(x >> 32);
+    const u32 bh = hw ? 1u : 0u, bo = K.one - bh;
+    u64 ah = z ? wh : (((u64)nhh << 32) | nhl), ao = ((u64)noh << 32) | nol;
+    ah = (u64)xl * bh + ah;
+    ao = (u64)xl * bo + ao;
+    wh = ((u64)((u32)(ah >> 32) + xh * bh) << 32) | (u32)ah;
+    wo = ((u64)((u32)(ao >> 32) + xh * bo) << 32) | (u32)ao;
+    p = z ? (RULE ? lh + 1u : lh) : p - 1u;
+    lh = lh1 + (hw ? (z ? 1u : 2u) : 0u);
+    lo = lo1 + (hw ? 0u : 2u);
+    return lo == 0u;
+}
+
 // Path-memo key of a held-out state (the entry format of war_refill.cuh: the key itself is not stored, the
 // slot and entry give it back).  The n-1 other cards in the order holder's then opponent's, the holder's
 // count lh and the depth p; the last card is the one missing.  At 17 cards that is 15 nibbles + 8 bits =
@@ -169,7 +202,7 @@ __device__ __noinline__ void h_store_cycle(u64* T, u32 bits, u64 wh, u64 wo, u32
     }
 }
 
-template <int RULE, bool MEMO>
+template <int RULE, bool MEMO, bool FMA>
 __global__ void __launch_bounds__(MEMO ? 512 : 1024) held_kernel(const __grid_constant__ HeldArgs a,
                                                                 DevAcc* __restrict__ acc) {
     extern __shared__ u32 sh[];
@@ -179,6 +212,7 @@ __global__ void __launch_bounds__(MEMO ? 512 : 1024) held_kernel(const __grid_co
     __syncthreads();
 
     const u32 n = (u32)a.n, W = (u32)a.W;
+    const TurnK K = a.tk;
     const u32 hb1 = a.hbins > 0 ? (u32)(a.hbins - 1) : 0u;
     const int period = a.defer > 4 ? (a.defer + 3) & ~3 : 4;
     u64* counter = &acc->work_next;
@@ -217,7 +251,7 @@ __global__ void __launch_bounds__(MEMO ? 512 : 1024) held_kernel(const __grid_co
     bool running = __any_sync(WAR_FULL_MASK, active);
     while (running) {
         for (int k = 0; k < period; k++) {
-            bool en = h_turn<RULE>(wh, wo, lh, lo, p);
+            bool en = FMA ? h_turn_fma<RULE>(wh, wo, lh, lo, p, K) : h_turn<RULE>(wh, wo, lh, lo, p);
             if (!done) rounds++;
             const bool cy = (wh == th) & (wo == to) & (lh == tlh) & (p == tp);
             en = en | (lo == 0u);
@@ -299,23 +333,25 @@ __global__ void __launch_bounds__(MEMO ? 512 : 1024) held_kernel(const __grid_co
 
 typedef void (*HeldFn)(const HeldArgs, DevAcc*);
 
-static HeldFn held_pick(int rule, bool memo) {
-    if (rule) return memo ? held_kernel<1, true> : held_kernel<1, false>;
-    return memo ? held_kernel<0, true> : held_kernel<0, false>;
+static HeldFn held_pick(int rule, bool memo, bool fma) {
+    if (rule) return memo ? (fma ? held_kernel<1, true, true> : held_kernel<1, true, false>)
+                          : (fma ? held_kernel<1, false, true> : held_kernel<1, false, false>);
+    return memo ? (fma ? held_kernel<0, true, true> : held_kernel<0, true, false>)
+                : (fma ? held_kernel<0, false, true> : held_kernel<0, false, false>);
 }
 
 cudaError_t launch_held(const HeldArgs& a, int threads, int blocks, DevAcc* acc, cudaStream_t st) {
     const size_t shmem = sizeof(u32) * (size_t)(a.hbins + WAR_EBINS);
-    held_pick(a.rule, a.memo != nullptr)<<<blocks, threads, shmem, st>>>(a, acc);
+    held_pick(a.rule, a.memo != nullptr, a.fma != 0)<<<blocks, threads, shmem, st>>>(a, acc);
     note_launch();
     return cudaGetLastError();
 }
 
-int held_max_blocks_per_sm(int rule, int threads, int hbins, bool memo) {
+int held_max_blocks_per_sm(int rule, int threads, int hbins, bool memo, bool fma) {
     if (memo && threads > 512) return 0;
     int nb = 0;
     const size_t shmem = sizeof(u32) * (size_t)(hbins + WAR_EBINS);
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, held_pick(rule, memo), threads, shmem);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, held_pick(rule, memo, fma), threads, shmem);
     return e == cudaSuccess ? nb : 0;
 }
 

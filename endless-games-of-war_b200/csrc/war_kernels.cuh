@@ -136,10 +136,12 @@ struct HeldArgs {
     const Unit* units;
     int n, m, rule, hbins, W, defer;
     u64* memo;        // path memo (2^memo_bits words, 0 = empty), or null
-    u32 memo_bits, pad;
+    u32 memo_bits;
+    int fma;          // the multiply-add, branch-free turn (h_turn_fma)
+    TurnK tk;         // its constants
 };
 cudaError_t launch_held(const HeldArgs& a, int threads, int blocks, DevAcc* acc, cudaStream_t st);
-int held_max_blocks_per_sm(int rule, int threads, int hbins, bool memo);
+int held_max_blocks_per_sm(int rule, int threads, int hbins, bool memo, bool fma);
 
 struct FloydArgs {
     u64 fact[17];

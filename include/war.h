@@ -193,9 +193,9 @@ typedef struct war_job_status {
  * so it is kept out of the packed piles and tracked by its depth in its holder's pile; that keeps 17
  * cards in 4-bit nibbles.  Same job and result as war_enumerate for deals (cycling count, longest ending
  * game, cycle-length and ending-length histograms, turns), both rules; only WAR_F_MEMO_KEEP applies.
- * tune: threads, blocks_per_sm, block_m, window, defer; variant bit 2 = the path memo with memo_bits
- * (0 = 28), at most 512 threads then; NULL = defaults (no memo).  war_enumerate sends n = 17 deal jobs
- * here. */
+ * tune: threads, blocks_per_sm, block_m, window, defer; variant bit 0 = a branch-free multiply-add turn
+ * (same results, measured the same speed), bit 2 = the path memo with memo_bits (0 = 28), at most 512
+ * threads then; NULL = defaults (no memo).  war_enumerate sends n = 17 deal jobs here. */
 int war_enumerate_held(const war_job* job, const war_tune* tune, war_result* out);
 
 /* Coordinate descent over war_tune for the class of `job` (block_m, games, threads, blocks per SM, window,

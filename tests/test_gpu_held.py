@@ -20,10 +20,11 @@ def oracle_held(oracle, n, rule=0, lo=0, hi=None, hbins=128):
     return oracle.to_dict(oracle.enumerate_held(oracle.make_job(n, 0, rule, 0, lo, hi, hbins)))
 
 
-@pytest.mark.parametrize("rule", [0, 1])
-def test_small_n_full_against_oracle_and_main_engine(wl, oracle, rule):
+@pytest.mark.parametrize("rule,variant", [(0, 0), (1, 0), (0, 1), (1, 1)])
+def test_small_n_full_against_oracle_and_main_engine(wl, oracle, rule, variant):
+    """Every deal of n <= 11, both turn forms of the held-out engine (variant 1: multiply-add, branch-free)."""
     for n in range(2, 12):
-        got = held(wl, n, rule)
+        got = held(wl, n, rule, tune=wl.make_tune(variant=variant))
         want = oracle_held(oracle, n, rule)
         main = wl.to_dict(wl.enumerate_job(wl.make_job(n, rule=rule, hbins=128)))
         for k in FIELDS:
@@ -70,7 +71,9 @@ def test_n17_through_war_enumerate_and_tunes(wl, oracle):
     for k in FIELDS:
         assert got[k] == want[k], k
     for t in (dict(threads=128), dict(threads=1024, defer=4), dict(block_m=3, defer=16), dict(block_m=8, window=1),
-              dict(blocks_per_sm=1, window=128)):
+              dict(blocks_per_sm=1, window=128), dict(variant=1), dict(variant=1, threads=1024, rule=0),
+              dict(variant=5, memo_bits=20)):
+        t.pop("rule", None)
         got = held(wl, 17, 0, lo, hi, 256, wl.make_tune(**t))
         for k in FIELDS:
             assert got[k] == want[k], (t, k)
