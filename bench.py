@@ -1,19 +1,25 @@
 """Benchmark of the exhaustive War enumerator on B200.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload deals13|canon14|deals11] [--impl ours|reference]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload deals13|canon14|deals11|deals13slice]
+                    [--impl ours|reference] [--peaks]
 
 One step = one complete enumeration of the workload's rank space by the persistent refill kernel
-(war_enumerate), results checked bit-exactly against the reference's recorded values after the timed
-region.  Workloads (the rank spaces are the inputs; nothing is random):
+(war_enumerate), every step checked bit-exactly against the reference's recorded values.  Workloads (the
+rank spaces are the inputs; nothing is random):
   deals13  all 13! = 6,227,020,800 deals, cycle-length and ending-length histograms   (default)
   canon14  all 13!*13 = 80,951,270,400 canonical positions of n = 14, distinct cycles, cycle-length
            histogram and the seeded 1% Floyd cross-check
   deals11  all 11! deals (plain GPU drop-in size)
+The default line also carries the rest of the headline metric, measured after the timed region: the
+batched-versus-plain ratio (the plain kernel on the same job), `canon14` (the reference's long run
+`war_gpu.py 14 --canon --distinct --shape --hist 256` with the 1% Floyd sample, bit-exact against
+data/long_runs.txt:20-23) and `serving` (a seeded Poisson stream of jobs below the server's capacity:
+throughput, p50 / p99 job latency, every job checked against the plain kernel).
 With N ranks (torchrun, one GPU each) the rank space is cut into N contiguous shards and the per-rank
 results are summed with one all-reduce of the accumulators (strong scaling).  Rank 0 prints one JSON
 line.  --impl reference times the reference's own CPU program (cpu/war.cpp, built unmodified into
-oracle/_ref/) or, when a full run would not fit the time budget, the oracle's restatement of it on a
-bounded strided sample, on all host cores.
+oracle/_ref/) over the whole workload once, and the oracle's restatement of it on bounded strided
+samples, on all host cores.  --peaks prints the measured ceilings (integer issue, random gathers) alone.
 """
 import argparse
 import json
@@ -35,6 +41,10 @@ K_OPS_PER_TURN = 30
 # DRAM bytes (read + write) per deal of the path-memo refill kernel, from an ncu capture of the second span
 # of `war_gpu.py 13 --hist 256` (1.94e9 deals, 214.6 GB): the random memo reads cost ~108 B each.
 MEMO_DRAM_BYTES_PER_DEAL = 110.8
+# Turns of the reference's own schedule (Brent with the tortoise saved at powers of two from the first turn)
+# over all 13! deals, as counted by an instrumented copy of cpu/war.cpp; the plain kernel reproduces it
+# exactly (its `turns`).
+REF_SCHEDULE_TURNS = {13: 686746920144}
 
 WORKLOADS = {
     "deals13": dict(n=13, mode=0, hbins=256, flags=0, label="n=13 all deals (war_gpu.py 13 --hist 256)"),
@@ -139,7 +149,14 @@ def max_over_ranks(x, ws):
 
 
 def reference_arm(args, rank, ws):
-    """The reference's CPU implementation on the host cores (rank 0 only)."""
+    """The reference's CPU implementation on the host cores (rank 0 only).
+
+    Deals: the reference's own cpu/war.cpp (built unmodified into oracle/_ref/) over the whole workload once,
+    `war 13 0` (about 70 s on 16 threads); its rate is the line's value.  Beside it, the oracle's restatement
+    of the same algorithm is timed on bounded strided samples for the requested steps (each a few seconds),
+    and its calibration against the full run is reported.  Canonical positions: the reference has no CPU
+    program that fits the time (cpu/distinct_cycles.c takes tens of minutes at n = 14), so the samples of the
+    restatement are the value."""
     if rank != 0:
         return
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
@@ -148,47 +165,45 @@ def reference_arm(args, rank, ws):
     n, mode = w["n"], w["mode"]
     cores = os.cpu_count() or 1
     total = space(n, mode)
-    line = {"impl": "reference", "metric": "positions/s" if mode else "deals/s", "unit": "positions/s" if mode else "deals/s",
-            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
-            "scaling": "strong", "vs_baseline": None, "dtype": "u64", "data": "exhaustive (deterministic rank space)",
+    unit = "positions/s" if mode else "deals/s"
+    line = {"impl": "reference", "metric": unit, "unit": unit, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "u64", "data": "exhaustive (deterministic rank space)",
             "config": {"workload": w["label"], "n": n, "mode": "canon" if mode else "deals"}}
-    use_ref = (mode == 0 and oracle.ref_available("war"))
-    est = None
-    if use_ref:
+    full = None
+    if mode == 0 and "lo" not in w and oracle.ref_available("war"):
+        oracle.ref_war(min(n, 11), 0)                                  # warm-up: page cache, thread pool
         t0 = time.time()
-        oracle.ref_war(11, 0)
-        t11 = time.time() - t0
-        # n = 13 plays 156x the deals of n = 11 at 3.6x the turns per deal (Brent turn totals)
-        est = t11 * (math.factorial(n) * (686746920144 / 6227020800)) / (39916800 * 30.46)
-        use_ref = est * args.steps <= 240
-    times = []
-    if use_ref:
-        for _ in range(args.steps):
-            t0 = time.time()
-            deals, cyc, longest = oracle.ref_war(n, 0)
-            times.append(time.time() - t0)
-        assert deals == total
-        sample, kind, units = "full run of cpu/war.cpp %d 0 (%d deals)" % (n, total), "reference", total
+        deals, cyc, longest = oracle.ref_war(n, 0)
+        t_full = time.time() - t0
+        assert deals == total, (deals, total)
+        full = {"value": total / t_full, "seconds": t_full, "cores": cores, "cycling": cyc, "longest": longest,
+                "sample": "full run of the unmodified cpu/war.cpp: war %d 0 (%d deals)" % (n, total)}
+    # bounded strided samples of the same rank space with the restatement, ~60 s in all
+    per_step = 60.0 / max(1, args.steps + 1)
+    _oracle_sample_rate(w, min(per_step, 5.0), cores)                   # warm-up
+    times, done_units = [], 0
+    for s in range(args.steps):
+        v, slice_len = _oracle_sample_rate(w, per_step, cores, seed=s + 1)
+        times.append(slice_len * 64 / v)
+        done_units += slice_len * 64
+    port = done_units / sum(times)
+    port_line = {"value": port, "steps": args.steps, "ms_per_step": sum(times) / len(times) * 1e3,
+                 "sample": "64 strided slices of %d ranks of the %s space per step, oracle/war_oracle.c "
+                           "(restatement of the reference algorithm, OpenMP on all host threads)" % (
+                               slice_len, "canonical-position" if mode else "deal")}
+    if full:
+        v, t = full["value"], full["seconds"]
+        port_line["calibration_vs_reference"] = port / v
+        line.update({"steps": 1, "steps_requested": args.steps, "warmup": 1, "value": v, "ms_per_step": t * 1e3,
+                     "cpu_baseline": {"value": v, "unit": unit, "cores": cores, "kind": "reference",
+                                      "sample": full["sample"]},
+                     "reference_full": full, "port_samples": port_line})
     else:
-        # bounded strided samples of the same rank space, ~150 s in all
-        per_step = 150.0 / max(1, args.steps + 1)
-        _oracle_sample_rate(w, min(per_step, 10.0), cores)           # warm-up
-        done_units = 0
-        for s in range(args.steps):
-            v, slice_len = _oracle_sample_rate(w, per_step, cores, seed=s + 1)
-            times.append(slice_len * 64 / v)
-            done_units += slice_len * 64
-        units = done_units / len(times)
-        sample, kind = ("64 strided slices of %d ranks of the %s space per step (oracle restatement of the "
-                        "reference algorithm; a full cpu/war.cpp run is estimated at %s s here)" % (
-                            slice_len, "canonical-position" if mode else "deal",
-                            "%.0f" % est if est else "n/a"), "port")
-    t = sum(times) / len(times)
-    v = units / t
-    line.update({"value": v, "ms_per_step": t * 1e3,
-                 "cpu_baseline": {"value": v, "unit": line["unit"], "cores": cores, "kind": kind, "sample": sample,
-                                  "estimate_full_s": est},
-                 "e2e": {"value": v, "unit": line["unit"], "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}})
+        line.update({"value": port, "ms_per_step": port_line["ms_per_step"],
+                     "cpu_baseline": {"value": port, "unit": unit, "cores": cores, "kind": "port",
+                                      "sample": port_line["sample"]}})
+    line["e2e"] = {"value": line["value"], "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
     print(json.dumps(line), flush=True)
 
 
@@ -227,6 +242,84 @@ def cpu_baseline(w, target_s=12.0):
                           slice_len, "canonical-position" if mode else "deal", target_s)}
 
 
+def peaks(warlib, table_bits, clk_mhz=None):
+    """The measured ceilings on this GPU: integer issue (LOP3+IMAD), the ALU pipe alone, random 8-byte and
+    32-byte gathers from a table of 2^table_bits words, and the nominal issue rate (SMs x 4 schedulers x 32
+    lanes x SM clock)."""
+    issue, alu = warlib.measure_int_peak()
+    info = warlib.device_info()
+    clk = clk_mhz or info.clock_mhz
+    return {"int_issue_ops_per_s": issue, "alu_ops_per_s": alu,
+            "nominal_issue_ops_per_s": info.sm_count * 4 * 32 * clk * 1e6, "sm_count": info.sm_count,
+            "clock_mhz": clk, "gather_table_bytes": 8 << table_bits,
+            "gather8_lookups_per_s": warlib.measure_gather_peak(table_bits, 8),
+            "gather32_lookups_per_s": warlib.measure_gather_peak(table_bits, 32)}
+
+
+def canon14_leg(warlib, war_gpu, golden, stream):
+    """The reference's long run `war_gpu.py 14 --canon --distinct --shape --hist 256` (data/long_runs.txt:20-23)
+    with the seeded 1% sample of the north-star's canonical configuration: every canonical position of n = 14
+    once per rep through war_enumerate (device time, CUDA events on the launching stream), checked
+    bit-exactly, then the sample replayed with Floyd and compared with Brent's aggregates."""
+    import torch
+    F = warlib.F_DISTINCT | warlib.F_SHAPE | warlib.F_SAMPLE
+    tune = war_gpu._tune_for(14, True, 0, F)
+    job = warlib.make_job(14, warlib.CANON, 0, F, hbins=256, dbins=4096, sample_ppm=10000, seed=14)
+    warlib.enumerate_job(warlib.make_job(14, warlib.CANON, 0, F, 0, 10 ** 8, hbins=256, dbins=4096,
+                                         sample_ppm=10000, seed=14), tune)        # untimed: first launch
+    g = golden["canon_rule0"]["14"]
+    dh = {int(k): v for k, v in g["dhist"].items()}
+    hh = {int(k): v for k, v in g["hist"].items()}
+    ms = []
+    for _ in range(2):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        r = warlib.enumerate_job(job, tune)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms.append(e0.elapsed_time(e1))
+        d = warlib.to_dict(r)
+        ok = ((d["cyc"], d["done"], d["maxfin"], d["distinct_min"], d["dhist"], d["hist"], d["shape_nonstd"],
+               d["shape_unchecked"]) == (g["cycling"], g["positions"], g["longest"], g["distinct"], dh, hh,
+                                         g["shape_nonstd"], g["shape_unchecked"]))
+        if not ok:
+            raise SystemExit("canon14 RESULT MISMATCH: %r" % ({k: d[k] for k in ("cyc", "done", "maxfin")},))
+    f = warlib.floyd_sample(job)
+    key = lambda x: (x.s_count, x.s_cyc, x.s_lamsum, x.s_lensum, x.s_maxfin)
+    if key(f) != key(r):
+        raise SystemExit("canon14 Floyd sample disagrees with Brent")
+    t = min(ms)
+    return {"workload": "n=14 canonical positions, war_gpu.py 14 --canon --distinct --shape --hist 256, "
+                        "1% seeded Floyd sample", "positions": g["positions"], "value": g["positions"] / (t * 1e-3),
+            "unit": "positions/s", "ms": t, "ms_reps": ms, "floyd_sample_ms": f.kernel_ms,
+            "floyd_sample_positions": f.s_count, "turns": r.turns, "memo_hit_rate": r.memo_hits / max(1, r.memo_lookups),
+            "check": "bit-exact vs data/long_runs.txt:20-23 (cycling, longest, distinct, weights, shape, lengths); "
+                     "Floyd sample = Brent sample",
+            "reference_published_s": 596.6, "tune": {k: getattr(tune, k) for k, _ in tune._fields_}}
+
+
+def serving_leg(warlib, jobs, rate, seed=2026):
+    """A seeded Poisson stream of the serving workload below the server's capacity: throughput over the
+    stream, job latency (submit to result) percentiles, and every job against the plain kernel."""
+    import serve
+    stream = serve.poisson_stream(jobs, rate, seed)
+    with serve.Server() as s:
+        results, lat, wall = serve.serve_stream(stream, s)
+        st = s.stats()
+        mi = s.memo_info()
+    ranks = sum(j.hi - j.lo for _, j in stream)
+    t0 = time.time()
+    bad = serve.verify(stream, results)
+    return {"workload": "serving: %d seeded Poisson jobs at %.0f/s (n uniform over 9,10,11,13,14,15; 70%% deals; "
+                        "20%% loser-first; half of the canonical jobs --distinct; log-uniform 1e4..1e9 ranks)"
+                        % (jobs, rate),
+            "jobs": jobs, "ranks": ranks, "wall_s": wall, "offered_ranks_per_s": ranks / stream[-1][0],
+            "ranks_per_s": ranks / wall, "latency_ms": {"p50": serve.percentile(lat, 50),
+                                                        "p99": serve.percentile(lat, 99), "max": max(lat)},
+            "server": st, "memo_arena": mi, "mismatches_vs_plain": bad, "verify_s": time.time() - t0}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -237,6 +330,12 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the plain-kernel comparison run")
+    ap.add_argument("--no-canon14", action="store_true", help="skip the n = 14 canonical leg")
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving leg")
+    ap.add_argument("--serving-jobs", type=int, default=600)
+    ap.add_argument("--serving-rate", type=float, default=20.0)
+    ap.add_argument("--peaks", action="store_true", help="print the measured ceilings only")
+    ap.add_argument("--table-bits", type=int, default=30, help="--peaks: gather table of 2^bits words")
     args = ap.parse_args()
 
     rank, ws, local = dist_init()
@@ -250,6 +349,11 @@ def main():
     import torch
     import warlib
     import war_gpu
+    if args.peaks:
+        print(json.dumps(peaks(warlib, args.table_bits)), flush=True)
+        return
+    with open(os.path.join(ROOT, "tests", "golden", "golden.json")) as f:
+        golden = json.load(f)
     w = WORKLOADS[args.workload]
     n, mode = w["n"], w["mode"]
     import shard
@@ -293,18 +397,18 @@ def main():
     ms_max = max_over_ranks(ms, ws)
     kernel_ms = sum(r.kernel_ms for r in results) / len(results)
     turns = results[-1].turns
-    # exactness of every step
-    for r in results:
-        assert r.done == results[0].done and r.cyc == results[0].cyc and r.maxfin == results[0].maxfin
     res = results[-1]
-    acc = [res.cyc, res.done, res.maxfin, res.turns, res.distinct_min, res.oncycle]
-    if ws > 1:   # the one exchange of the sharded path: combine the per-rank results
-        import shard
-        d = shard.allreduce_result(shard.result_to_dict(res), device="cuda")
-        acc = [d["cyc"], d["done"], d["maxfin"], d["turns"], d["distinct_min"], d["oncycle"]]
-    check = verify(w, acc, res if ws == 1 else None) if "lo" not in w else "slice (no recorded total)"
+    check = "slice (no recorded total)"
+    for r in results:                  # every timed step, bit-exact
+        acc = [r.cyc, r.done, r.maxfin, r.turns, r.distinct_min, r.oncycle]
+        if ws > 1:   # the one exchange of the sharded path: combine the per-rank results
+            d = shard.allreduce_result(shard.result_to_dict(r), device="cuda")
+            acc = [d["cyc"], d["done"], d["maxfin"], d["turns"], d["distinct_min"], d["oncycle"]]
+        if "lo" not in w:
+            check = verify(w, acc, r if ws == 1 else None, golden)
 
-    # e2e through the public drop-in API (war_gpu.run), host buffers, copies inside the timed region
+    # e2e through the public drop-in API (war_gpu.run), host structs in, host results out, every copy inside
+    # the timed region; its result is checked against the recorded one
     e2e = None
     if not args.no_e2e:
         kw = dict(hbins=w["hbins"], canon=mode == 1, dbins=w.get("dbins", 0), quiet=True)
@@ -312,7 +416,12 @@ def main():
 
         def e2e_step():
             if ws == 1 and "lo" not in w:
-                war_gpu.run(n, **kw)
+                out = war_gpu.run(n, **kw)
+                dmin = sum(v // k for k, v in out[6].items()) if out[6] else None
+                verify(w, [out[0], out[1], out[2], None, dmin, None], None, golden)
+                if mode == 0:
+                    g = golden["deals_rule0"][str(n)]
+                    assert {str(k): v for k, v in out[4].items()} == g["hist"], "e2e histogram mismatch"
             else:
                 warlib.enumerate_job(job, tune)
         e2e_step()                      # untimed: first-call set-up of the Python side
@@ -325,56 +434,88 @@ def main():
         torch.cuda.synchronize()
         barrier(ws)
         e2e_s = max_over_ranks((time.perf_counter() - t0) / reps, ws)
-        h2d = 64 + 24 * 64 + 512       # job/tune structs, extra units, kernel parameter block per launch
-        d2h = 73880                      # the accumulator block read back per launch
+        # per step: the extra work units copied in for each engine call, and the accumulator block read back
+        spans = []
+        if ws == 1 and "lo" not in w:
+            mult = (n - 1) if mode else 1
+            orders = hi0 // mult
+            span = max(war_gpu.SPAN_RANKS // mult, 1)
+            spans = [(a * mult, min(orders, a + span) * mult) for a in range(0, orders, span)]
+        else:
+            spans = [(lo, hi)]
+        h2d = 0
+        for a, b in spans:
+            h2d += 24 * len(warlib.plan(warlib.make_job(n, mode, 0, w["flags"], a, b), tune.block_m if tune else 6)[2])
+        d2h = 73880 * len(spans)
         e2e = {"value": total / e2e_s, "unit": "positions/s" if mode else "deals/s", "h2d_bytes_per_step": h2d,
-               "d2h_bytes_per_step": d2h, "api": "war_gpu.run" if ws == 1 else "warlib.enumerate_job"}
+               "d2h_bytes_per_step": d2h, "api": "war_gpu.run" if ws == 1 else "warlib.enumerate_job",
+               "check": "result tuple equal to the recorded one" if ws == 1 and "lo" not in w else None}
 
     # the plain kernel (the reference's per-thread rank blocks, restated for sm_100a) on the same job,
     # once, outside the timed region: the batched-versus-plain ratio
     plain = None
+    warlib.set_stream(stream.cuda_stream)
     if not args.no_plain and ws == 1:
-        warlib.set_stream(stream.cuda_stream)
         rp = warlib.enumerate_plain(job)
         assert (rp.cyc, rp.done, rp.maxfin) == (res.cyc, res.done, res.maxfin), "plain and refill kernels disagree"
         plain = {"value": (hi - lo) / (rp.kernel_ms * 1e-3), "kernel_ms": rp.kernel_ms, "turns": rp.turns,
                  "batched_over_plain": rp.kernel_ms / kernel_ms}
 
+    c14 = None
+    if rank == 0 and ws == 1 and args.workload == "deals13" and not args.no_canon14:
+        c14 = canon14_leg(warlib, war_gpu, golden, stream)
+    serving = None
+    if rank == 0 and ws == 1 and args.workload == "deals13" and not args.no_serving:
+        serving = serving_leg(warlib, args.serving_jobs, args.serving_rate)
+
     if rank == 0:
-        issue_peak, alu_peak = warlib.measure_int_peak()
+        cs = clk.summary()
+        pk = peaks(warlib, (tune.memo_bits or 24) if tune is not None and (tune.variant & 4) else 30,
+                   clk_mhz=cs["sm_mhz"])
+        issue_peak, alu_peak, nominal = pk["int_issue_ops_per_s"], pk["alu_ops_per_s"], pk["nominal_issue_ops_per_s"]
         achieved = turns * K_OPS_PER_TURN / (kernel_ms * 1e-3)    # algorithmic int ops/s of the refill kernel
         memo = None
         if tune is not None and (tune.variant & 4) and res.memo_lookups:
             # the cycle memo's own traffic: one 8-byte word read per lookup, one written per store
             hbm_peak, hbm_src = measured_hbm_peak()
             mbytes = 8.0 * (res.memo_lookups + res.memo_stores)
+            lps = res.memo_lookups / (kernel_ms * 1e-3)
             memo = {"variant": tune.variant, "table_bytes": 8 << (tune.memo_bits or 24),
                     "lookups_per_game": res.memo_lookups / res.done, "hit_rate": res.memo_hits / res.memo_lookups,
                     "stores_per_game": res.memo_stores / res.done, "turns_per_game": res.turns / res.done,
+                    "lookups_per_s": lps, "gather_peak_lookups_per_s": pk["gather8_lookups_per_s"],
+                    "frac_of_gather_peak": lps / pk["gather8_lookups_per_s"],
+                    "algorithmic_bytes_per_lookup": 8,
+                    "dram_bytes_per_deal": MEMO_DRAM_BYTES_PER_DEAL if mode == 0 and n == 13 else None,
                     "algorithmic_GBps": mbytes / (kernel_ms * 1e-3) / 1e9, "hbm_peak_GBps": hbm_peak,
                     "frac_of_hbm": mbytes / (kernel_ms * 1e-3) / 1e9 / hbm_peak, "hbm_peak_source": hbm_src}
         unit = "positions/s" if mode else "deals/s"
         value = total * args.steps / (ms_max * 1e-3)
-        cs = clk.summary()
+        step_s = ms_max * 1e-3 / args.steps
         line = {
             "metric": unit, "value": value, "unit": unit, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
             "dtype": "u64 (4-bit packed cards, integer only)", "data": "exhaustive rank space (deterministic, no sampling)",
             "config": {"workload": w["label"], "n": n, "mode": "canon" if mode else "deals", "ranks": total,
                        "parallelism": "shard%d" % ws, "l2": "working set in registers; no per-step input (L2 flush n/a)"},
-            "turns_per_s": turns * ws / (ms_max * 1e-3 / args.steps),
+            "turns_per_s": turns * ws / step_s,
             "turns_per_step": turns * ws,
+            "turns_ref_schedule_per_s": (REF_SCHEDULE_TURNS[n] / step_s if mode == 0 and n in REF_SCHEDULE_TURNS
+                                         and "lo" not in w else None),
             "kernel_ms": kernel_ms,
             "floyd_check_ms": (sum(floyd_ms[-args.steps:]) / args.steps) if floyd_ms else None,
             "gpu_launches": launches,
             "roofline": {"bound": "int_issue", "achieved": achieved / 1e12, "peak": issue_peak / 1e12,
                          "unit": "Tops/s (INT32 thread-ops)", "frac": achieved / issue_peak,
+                         "peak_nominal": nominal / 1e12, "frac_of_nominal": achieved / nominal,
                          "alu_pipe_peak": alu_peak / 1e12, "frac_of_alu_pipe": achieved / alu_peak,
-                         "ops_per_turn": K_OPS_PER_TURN,
+                         "ops_per_turn": K_OPS_PER_TURN, "turns_per_launch": turns / max(1, launches // args.steps),
                          "traffic": (MEMO_DRAM_BYTES_PER_DEAL * total / max(1, launches // args.steps)
                                      if memo and mode == 0 and n == 13 else None),
                          "traffic_unit": "DRAM bytes per launch (ncu capture scaled by deals per launch)",
-                         "peak_source": "war_measure_int_peak on this GPU (LOP3+IMAD issue ceiling)"},
+                         "peak_source": "war_measure_int_peak on this GPU (LOP3+IMAD issue ceiling, measured); "
+                                        "nominal = SMs x 4 x 32 x median SM clock"},
+            "peaks": pk,
             "clocks": cs,
             "check": check,
             "tune": {k: getattr(tune, k) for k, _ in tune._fields_} if tune is not None else None,
@@ -385,6 +526,10 @@ def main():
             line["e2e"] = e2e
         if plain:
             line["plain_kernel"] = plain
+        if c14:
+            line["canon14"] = c14
+        if serving:
+            line["serving"] = serving
         if not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(w)
         print(json.dumps(line), flush=True)
@@ -393,10 +538,8 @@ def main():
         dist.destroy_process_group()
 
 
-def verify(w, acc, res):
+def verify(w, acc, res, g):
     """Bit-exact check against the reference's recorded values (data/checks.txt, data/long_runs.txt)."""
-    with open(os.path.join(ROOT, "tests", "golden", "golden.json")) as f:
-        g = json.load(f)
     cyc, done, maxfin, turns, dmin, oncyc = acc
     n = w["n"]
     if w["mode"] == 0:

@@ -232,6 +232,22 @@ int resolve_tune(const war_job* job, const war_tune* in, Tune& t) {
 int floyd_sample_run(const war_job* job, war_result* out) {
     Ctx& c = ctx();
     cudaError_t e;
+    if (job->sample_ppm >= 1000000u) {   // every position: Floyd over the job's own enumeration, no buffer
+        FloydArgs a;
+        memset(&a, 0, sizeof a);
+        fill_fact(a.fact);
+        a.n = job->n; a.canon = job->mode == WAR_CANON; a.rule = job->rule;
+        a.half = (job->flags & WAR_F_HALF) ? 1 : 0;
+        a.per = 256;
+        a.seed = job->seed;
+        a.thr = 1ull << 32;
+        a.start = job->lo; a.total = job->hi;
+        const int blocks = c.sm_count * floyd_enum_blocks_per_sm(a.canon, a.rule);
+        int st = run_launch([&](cudaStream_t x) { return launch_floyd_enum(a, blocks, c.d_acc, x); }, &out->kernel_ms);
+        if (st) return st;
+        merge_acc(*c.h_acc, out, 0, 0);
+        return WAR_OK;
+    }
     if (!c.d_sample) {
         c.sample_cap = 1u << 22;   // 4M positions, 64 MB
         if ((e = cudaMalloc(&c.d_sample, sizeof(ulonglong2) * c.sample_cap)) != cudaSuccess) {
@@ -465,8 +481,11 @@ int war_enumerate_plain(const war_job* job, war_result* out) {
 }
 
 // The context's memo table for a job: 2^bits words, cleared unless the job asks to keep the table the
-// previous job of the same n, rule and key format (kind: 0 the main engine, 1 the held-out engine, 2 the
-// main engine's shape-carrying values) left.
+// previous job of the same n, rule and entry layout left.  kind names the layout: 1 the held-out engine;
+// for the main engine 4 * form + 2 * shape, with form 1 (landmarks, key | lam << shift), 2 (all cycle
+// states, same packing) or 3 (path entries, (key * C) << bits | value) and shape = 1 when cycle values
+// carry the loop-shape code.  Two layouts never share a table: an entry of one form read as another could
+// name a different state.
 static int prepare_memo(Ctx& c, const war_job* job, int bits, int kind, u64** table) {
     cudaError_t e;
     const size_t bytes = sizeof(u64) << bits;
@@ -612,8 +631,10 @@ int war_enumerate(const war_job* job, const war_tune* tune, war_result* out) {
     a.thr = ((u64)job->sample_ppm << 32) / 1000000u;
     a.units = c.d_units;
     if (t.variant & 4) {   // the cycle memo
-        // kind 2: the shape-carrying values of a canonical scan with the loop-shape test
-        const int kind = (job->mode == WAR_CANON && (job->flags & WAR_F_SHAPE)) ? 2 : 0;
+        // its entry layout: the form the variant selects, and the shape-carrying values of a canonical scan
+        // with the loop-shape test
+        const int form = (t.variant & 24) == 24 ? 3 : ((t.variant & 8) ? 2 : 1);
+        const int kind = 4 * form + ((job->mode == WAR_CANON && (job->flags & WAR_F_SHAPE)) ? 2 : 0);
         if ((st = prepare_memo(c, job, t.memo_bits, kind, &a.memo))) return st;
         a.memo_bits = (u32)t.memo_bits;
     }

@@ -21,7 +21,7 @@ struct Ctx {
     u64* d_memo = nullptr;          // cycle memo table of the refill kernel (deals)
     int memo_bits = 0;
     int memo_n = -1, memo_rule = -1;  // job class whose cycles the memo holds
-    int memo_kind = 0;                // its key format: 0 the main engine, 1 the held-out engine
+    int memo_kind = 0;                // its entry layout (prepare_memo): engine, memo form, shape values
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
 };
 
@@ -52,6 +52,8 @@ int floyd_sample_run(const war_job* job, war_result* out);
 
 cudaError_t launch_sample_scan(const FloydArgs& a, int threads, u64 nthreads, ulonglong2* buf, u64 cap, DevAcc* acc,
                                cudaStream_t st);
+cudaError_t launch_floyd_enum(const FloydArgs& a, int blocks, DevAcc* acc, cudaStream_t st);
+int floyd_enum_blocks_per_sm(int canon, int rule);
 cudaError_t launch_floyd_play(const ulonglong2* buf, u64 cap, int n, int rule, int blocks, int threads, DevAcc* acc,
                               cudaStream_t st);
 

@@ -14,7 +14,11 @@
 //
 // Jobs of the same n and rule share one cycle memo (war_refill.cuh): its entries are facts about n and the
 // rule, so every job of that class, now and later, decides its games from what the earlier ones found.
-// The tables are allocated when the first job of a class is admitted and kept until the server ends.
+// The tables come from one arena that war_server_create reserves inside the memory budget (after the
+// accumulator slots); a class takes its table from the arena when its first job is admitted, cleared on
+// the compute stream, and keeps it until the server ends.  The worker thread never calls cudaMalloc, which
+// would synchronise the device in the middle of the tick stream.  A class whose table no longer fits runs
+// without the memo.
 #include <cuda_runtime.h>
 #include <algorithm>
 #include <cmath>
@@ -123,6 +127,8 @@ struct war_server {
     std::map<uint64_t, war::SJob> jobs;
     std::vector<int> free_slots;
     std::map<std::pair<int, int>, std::pair<u64*, int>> memos;   // (n, rule) -> (table, log2 words)
+    u64* memo_arena = nullptr;      // reserved at create; tables are carved from it in admission order
+    u64 arena_words = 0, arena_used = 0;
     DevAcc* d_slots = nullptr;
     DevAcc* h_slot = nullptr;   // pinned readback buffer
     cudaStream_t s_comp = nullptr, s_copy = nullptr;
@@ -174,13 +180,19 @@ void set_args(war_server* s, SJob& J) {
         auto it = s->memos.find(cls);
         if (it == s->memos.end()) {
             const int cap = s->cfg.memo_bits ? s->cfg.memo_bits : 28;
-            const int bits = std::max(12, std::min(cap, 4 + (int)std::ceil(std::log2((double)fact(job.n)) * 0.75)));
+            int bits = std::max(12, std::min(cap, 4 + (int)std::ceil(std::log2((double)fact(job.n)) * 0.75)));
+            // the largest table of at most 2^bits words that the arena still holds (at least 2^12 words)
+            const u64 left = s->arena_words - s->arena_used;
+            while (bits >= 12 && (1ull << bits) > left) bits--;
             u64* t = nullptr;
-            if (cudaMalloc(&t, sizeof(u64) << bits) != cudaSuccess ||
-                cudaMemsetAsync(t, 0, sizeof(u64) << bits, s->s_comp) != cudaSuccess) {
-                if (t) cudaFree(t);
-                t = nullptr;
-                cudaGetLastError();   // no table: the class runs without the memo
+            if (bits >= 12) {
+                t = s->memo_arena + s->arena_used;
+                if (cudaMemsetAsync(t, 0, sizeof(u64) << bits, s->s_comp) != cudaSuccess) {
+                    t = nullptr;
+                    cudaGetLastError();   // not cleared: the class runs without the memo
+                } else {
+                    s->arena_used += 1ull << bits;
+                }
             }
             it = s->memos.emplace(cls, std::make_pair(t, bits)).first;
         }
@@ -430,6 +442,19 @@ int war_server_create(const war_server_cfg* cfg, war_server** out) {
         return fail(WAR_ENOMEM, "memory budget %llu holds no job accumulator (%zu bytes each)", (unsigned long long)budget,
                     sizeof(DevAcc));
     }
+    // the memo arena: what the budget leaves after the slots, at most 16 GiB, reserved now so that the
+    // worker thread never allocates; a smaller one when the device cannot give that much
+    if (c.memo_bits >= 0) {
+        const u64 rest = budget - (u64)s->nslots * sizeof(DevAcc);
+        u64 words = std::min<u64>(rest / sizeof(u64), 1ull << 31);
+        while (words >= (1ull << 12)) {
+            if (cudaMalloc(&s->memo_arena, words * sizeof(u64)) == cudaSuccess) break;
+            s->memo_arena = nullptr;
+            cudaGetLastError();
+            words /= 2;
+        }
+        s->arena_words = s->memo_arena ? words : 0;
+    }
     s->max_tasks = 16384;
     s->max_units = s->max_tasks + 4 * UNITS_PER_EXTRA_CAP;
     bool ok = cudaMalloc(&s->d_slots, sizeof(DevAcc) * (size_t)s->nslots) == cudaSuccess &&
@@ -516,6 +541,18 @@ int war_server_stats(war_server* s, uint64_t* ticks, uint64_t* jobs_done, uint64
     return WAR_OK;
 }
 
+int war_server_memo_info(war_server* s, uint64_t* arena_bytes, uint64_t* used_bytes, int32_t* classes) {
+    if (!s) return fail(WAR_EINVAL, "NULL server");
+    std::lock_guard<std::mutex> lk(s->mu);
+    int k = 0;
+    for (auto& kv : s->memos)
+        if (kv.second.first) k++;
+    if (arena_bytes) *arena_bytes = s->arena_words * sizeof(u64);
+    if (used_bytes) *used_bytes = s->arena_used * sizeof(u64);
+    if (classes) *classes = k;
+    return WAR_OK;
+}
+
 int war_server_destroy(war_server* s) {
     if (!s) return WAR_OK;
     {
@@ -536,8 +573,7 @@ int war_server_destroy(war_server* s) {
         if (T.d_units) cudaFree(T.d_units);
         if (T.ev) cudaEventDestroy(T.ev);
     }
-    for (auto& kv : s->memos)
-        if (kv.second.first) cudaFree(kv.second.first);
+    if (s->memo_arena) cudaFree(s->memo_arena);
     if (s->d_slots) cudaFree(s->d_slots);
     if (s->h_slot) cudaFreeHost(s->h_slot);
     if (s->s_comp) cudaStreamDestroy(s->s_comp);

@@ -6,7 +6,9 @@
 
 `poisson_stream()` draws the seeded job mix of the serving workload: n uniform over {9, 10, 11, 13, 14, 15},
 mode deals (p = 0.7) or canonical positions (p = 0.3), a rank range of log-uniform length in [1e4, 1e9]
-clipped to the space, at a uniform offset, arriving as a Poisson process.  `serve_stream()` replays such a
+clipped to the space, at a uniform offset, arriving as a Poisson process; a job plays the loser-first rule
+(--rule 1) with probability p_rule1 and a canonical job counts distinct cycles (--distinct) with
+probability p_distinct.  `serve_stream()` replays such a
 stream against a server in real time and reports throughput and job latencies (p50 / p99).
 
     python serve.py --jobs 2000 --rate 200 --verify
@@ -56,6 +58,13 @@ class Server:
                      "war_server_stats")
         return {"ticks": t.value, "jobs_done": d.value, "peak_resident": p.value}
 
+    def memo_info(self):
+        """The memo arena reserved at create, the bytes the job classes took from it, and their count."""
+        a, u, k = ctypes.c_uint64(), ctypes.c_uint64(), ctypes.c_int32()
+        warlib.check(warlib.lib().war_server_memo_info(self.h, ctypes.byref(a), ctypes.byref(u), ctypes.byref(k)),
+                     "war_server_memo_info")
+        return {"arena_bytes": a.value, "used_bytes": u.value, "classes": k.value}
+
     def wait_all(self, ids, timeout_s=600.0):
         """Results of the jobs, in order, waiting for each."""
         out = {}
@@ -89,7 +98,7 @@ class Server:
 
 
 def poisson_stream(count, rate, seed=2026, ns=(9, 10, 11, 13, 14, 15), p_deals=0.7, lmin=1e4, lmax=1e9,
-                   hbins=256):
+                   hbins=256, p_rule1=0.2, p_distinct=0.5, dbins=256):
     """[(arrival_s, job)] of the serving workload, seeded."""
     rnd = random.Random(seed)
     t = 0.0
@@ -102,7 +111,10 @@ def poisson_stream(count, rate, seed=2026, ns=(9, 10, 11, 13, 14, 15), p_deals=0
         length = int(math.exp(rnd.uniform(math.log(lmin), math.log(lmax))))
         length = max(1, min(length, total))
         lo = rnd.randrange(0, total - length + 1)
-        out.append((t, warlib.make_job(n, mode, 0, 0, lo, lo + length, hbins=hbins)))
+        rule = 1 if rnd.random() < p_rule1 else 0
+        distinct = mode == warlib.CANON and rnd.random() < p_distinct
+        out.append((t, warlib.make_job(n, mode, rule, warlib.F_DISTINCT if distinct else 0, lo, lo + length,
+                                       hbins=hbins, dbins=dbins if distinct else 0)))
     return out
 
 
@@ -140,13 +152,19 @@ def percentile(xs, p):
     return s[k]
 
 
+def same_result(p, r, job):
+    """Bit-exact equality of two results of one job (every count and histogram the job asks for)."""
+    return ((p.cyc, p.done, p.maxfin, p.oncycle, p.distinct_min, p.shape_nonstd, p.shape_unchecked) ==
+            (r.cyc, r.done, r.maxfin, r.oncycle, r.distinct_min, r.shape_nonstd, r.shape_unchecked) and
+            list(p.hist[:job.hbins]) == list(r.hist[:job.hbins]) and
+            list(p.dhist[:job.dbins]) == list(r.dhist[:job.dbins]) and list(p.endhist) == list(r.endhist))
+
+
 def verify(stream, results):
     """Every job's result against the plain kernel on the same range (bit-exact); returns mismatches."""
     bad = 0
     for (_, job), r in zip(stream, results):
-        p = warlib.enumerate_plain(job)
-        if (p.cyc, p.done, p.maxfin) != (r.cyc, r.done, r.maxfin) or list(p.hist[:job.hbins]) != list(r.hist[:job.hbins]) \
-                or list(p.endhist) != list(r.endhist):
+        if not same_result(warlib.enumerate_plain(job), r, job):
             bad += 1
     return bad
 

@@ -96,6 +96,7 @@ SYMBOLS = {
     "war_server_poll": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(Result), ctypes.POINTER(JobStatus)]),
     "war_server_drain": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_double]),
     "war_server_stats": (ctypes.c_int, [ctypes.c_void_p, U64P, U64P, U64P]),
+    "war_server_memo_info": (ctypes.c_int, [ctypes.c_void_p, U64P, U64P, ctypes.POINTER(ctypes.c_int32)]),
     "war_server_destroy": (ctypes.c_int, [ctypes.c_void_p]),
     "war_device_info_get": (ctypes.c_int, [ctypes.POINTER(DeviceInfo)]),
     "war_set_stream": (ctypes.c_int, [ctypes.c_void_p]),
@@ -103,6 +104,7 @@ SYMBOLS = {
     "war_launch_count": (ctypes.c_uint64, []),
     "war_sample_pick": (ctypes.c_int, [ctypes.c_uint64, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_uint64]),
     "war_measure_int_peak": (ctypes.c_int, [ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
+    "war_measure_gather_peak": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, ctypes.POINTER(ctypes.c_double)]),
     "war_plan": (ctypes.c_int, [ctypes.POINTER(Job), ctypes.c_int32, U64P, U64P, ctypes.POINTER(Unit), ctypes.c_int32]),
 }
 
@@ -250,6 +252,13 @@ def measure_int_peak():
     a, b = ctypes.c_double(), ctypes.c_double()
     check(lib().war_measure_int_peak(ctypes.byref(a), ctypes.byref(b)), "war_measure_int_peak")
     return a.value, b.value
+
+
+def measure_gather_peak(table_bits=30, bucket_bytes=8):
+    """Random lookups per second from a table of 2^table_bits words (war_measure_gather_peak)."""
+    v = ctypes.c_double()
+    check(lib().war_measure_gather_peak(table_bits, bucket_bytes, ctypes.byref(v)), "war_measure_gather_peak")
+    return v.value
 
 
 def set_stream(stream_handle):

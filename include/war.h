@@ -152,8 +152,11 @@ int war_enumerate(const war_job* job, const war_tune* tune, war_result* out);
 
 /* war_enumerate for callers that cannot allocate device memory: a host program whose own memory pool
  * has reserved the GPU (a cudaMalloc would fail or fragment it), or code on a latency-bound path that
- * cannot take cudaMalloc's implicit synchronisation.  No counterpart in the reference.  Same kernel,
- * arguments and results as war_enumerate (kernel_ms is host wall time here), but its scratch (one job's
+ * cannot take cudaMalloc's implicit synchronisation.  No counterpart in the reference.  Same refill
+ * kernel, arguments and results as war_enumerate for jobs of 1..16 cards (kernel_ms is host wall time
+ * here), with two differences: 17-card deals, which war_enumerate hands to the held-out engine, are
+ * refused with WAR_EINVAL, and the cycle memo is never used (tune.variant bits 2-4 are ignored, so
+ * memo_lookups stays 0), because its table would be allocated memory.  The scratch (one job's
  * accumulators and work counter, and at most 1024 extra work units; about 98 KB) lives in a static
  * device array that every GPU loading the library holds until exit; jobs whose plan needs more extra
  * units are refused with WAR_EINVAL.  The first call on each device looks up that array's address
@@ -162,10 +165,12 @@ int war_enumerate(const war_job* job, const war_tune* tune, war_result* out);
  * whose work overlaps on the GPU race. */
 int war_enumerate_noalloc(const war_job* job, const war_tune* tune, war_result* out);
 
-/* Floyd cross-check (the second detector of gpu/war_gpu_floyd.py:95-105): plays, with Floyd's
- * tortoise and hare, every position of the job whose seeded hash falls in the sample, and fills the
- * s_* fields of out (the rest is zero).  They must equal the s_* fields of war_enumerate /
- * war_enumerate_plain run with WAR_F_SAMPLE on the same job. */
+/* Floyd cross-check (the second detector of gpu/war_gpu_floyd.py:95-105 and cpu/war_floyd.c:14-63): plays,
+ * with Floyd's tortoise and hare, every position of the job whose seeded hash falls in the sample, and
+ * fills the s_* fields of out (the rest is zero).  They must equal the s_* fields of war_enumerate /
+ * war_enumerate_plain run with WAR_F_SAMPLE on the same job.  sample_ppm = 1000000 plays every position of
+ * the job (the full-range check: s_count = positions, s_cyc = cycling, s_maxfin = longest ending game),
+ * enumerated by its own lexicographic unrank and next-permutation. */
 int war_floyd_sample(const war_job* job, war_result* out);
 
 /* ---- serving: continuous batching of enumeration jobs (no reference counterpart) ----------- */
@@ -175,11 +180,17 @@ typedef struct war_server war_server;
 typedef struct war_server_cfg {
     int32_t max_jobs;        /* resident job slots (accumulator sets kept on the device) */
     int32_t queue_cap;       /* pending jobs the submit queue holds before WAR_EBUSY */
-    uint64_t mem_budget;     /* bytes of device memory the server may hold for job accumulators; 0 = free memory / 2 */
+    uint64_t mem_budget;     /* bytes of device memory the server may hold for job accumulators and cycle
+                                memos; 0 = free memory / 2.  The accumulator slots come first (max_jobs of
+                                them, or as many as fit); what is left, up to 16 GiB, is reserved at create
+                                as the memo arena, from which each job class takes its table when its first
+                                job is admitted (nothing is allocated after create) */
     uint64_t tick_ranks;     /* ranks issued per tick across all jobs (0 = default) */
     int32_t threads, blocks_per_sm;
     int32_t memo_bits;       /* cycle memo shared by all jobs of one n and rule, log2 of its 8-byte words
-                                (grown with n up to this; 0 = 28, i.e. 2 GiB per class; < 0 = no memo) */
+                                (grown with n up to this, shrunk to what the arena has left; 0 = 28, i.e.
+                                2 GiB per class; < 0 = no memo).  A class whose table does not fit runs
+                                without the memo, with the same results */
     int32_t reserved[3];
 } war_server_cfg;
 
@@ -216,6 +227,9 @@ int war_server_poll(war_server* s, uint64_t id, war_result* res, war_job_status*
 /* Waits (bounded by timeout_ms) until every submitted job is done. */
 int war_server_drain(war_server* s, double timeout_ms);
 int war_server_stats(war_server* s, uint64_t* ticks, uint64_t* jobs_done, uint64_t* peak_resident);
+/* The memo arena reserved at create (bytes), the part of it the job classes took so far, and how many
+ * classes have a table. */
+int war_server_memo_info(war_server* s, uint64_t* arena_bytes, uint64_t* used_bytes, int32_t* classes);
 int war_server_destroy(war_server* s);
 
 /* ---- utilities --------------------------------------------------------------------------------- */
@@ -244,6 +258,12 @@ int war_set_stream(void* cuda_stream);
  * IMAD alternating (ALU and FMA pipes, the issue-slot ceiling), alu = LOP3 only (the ALU pipe).  The
  * denominator of the roofline of the integer-bound enumeration kernels.  No reference counterpart. */
 int war_measure_int_peak(double* issue_ops_per_s, double* alu_ops_per_s);
+/* Measures random-gather throughput (lookups per second): independent loads of one 8-byte word
+ * (bucket_bytes = 8) or one aligned 32-byte bucket (32) at uniformly random positions of a table of
+ * 2^table_bits words (20..31; the cycle memo's table when it has that size, else one allocated for the
+ * call), eight in flight per thread.  The ceiling of the cycle memo's lookups, which are such loads.  No
+ * reference counterpart. */
+int war_measure_gather_peak(int32_t table_bits, int32_t bucket_bytes, double* lookups_per_s);
 /* Copies the last error message of the calling thread; returns its length. */
 int war_last_error(char* buf, size_t len);
 /* Kernels this library launched since load (its own kernels only). */

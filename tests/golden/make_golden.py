@@ -1,6 +1,7 @@
 """Writes tests/golden/golden.json from the reference's recorded outputs.
 
 Run it where the reference is mounted (read-only):  python tests/golden/make_golden.py [REF_ROOT]
+(REF_ROOT defaults to $WAR_REF, else the reference's mount point in the build container).
 The JSON is committed; nothing reads the reference at test time.  Sources (paths in the reference):
   data/deals.tsv                 a(n), longest ending game, cycle-length split, n = 1..17
   data/canonical_positions.tsv   canonical positions: entering a cycle, on a cycle, cycles
@@ -14,7 +15,7 @@ import os
 import re
 import sys
 
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("WAR_REF", "/root/reference")
 OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden.json")
 
 
@@ -122,7 +123,28 @@ def main():
             checks.split("== Canonical positions, distinct cycles and the Theorem-3 test, n = 1..13")[1].split("==")[0]),
         # gpu/war17.py 13 --nmin 5 (checks.txt:81-91)
         "war17_5_13": out_lines(checks.split("== Deals, 17-card GPU program")[1].split("==")[0]),
+        # war_gpu.py 14 --half --hist 256 (long_runs.txt:14-15)
+        "long14_half": out_lines(long_runs.split("python war_gpu.py 14 --half --hist 256;")[1].split("n=15")[0]),
+        # war_gpu.py 14 --canon --distinct --shape --hist 256 (long_runs.txt:20-23)
+        "long14_canon": out_lines(long_runs.split("python war_gpu.py 14 --canon --distinct --shape --hist 256")[1]
+                                  .split("$")[0]),
     }
+
+    # gpu/war24.py result lines (checks.txt:73-79, long_runs.txt:62-75)
+    w24 = []
+    for m in re.finditer(r"n=(\d+) det=(\w+) range=\[(\d+),(\d+)\) deals_simulated=(\d+) \(expected (\d+)\) "
+                         r"cycling=(\d+) longest_finite=(\d+) undetermined=(\d+)", checks + long_runs):
+        w24.append({"n": int(m.group(1)), "det": m.group(2), "lo": int(m.group(3)), "hi": int(m.group(4)),
+                    "deals": int(m.group(5)), "cyc": int(m.group(7)), "longest": int(m.group(8)),
+                    "undetermined": int(m.group(9)), "line": m.group(0)})
+    g["war24"] = w24
+
+    # gpu/war_gpu_floyd.py full-range deal runs without --half (long_runs.txt:35, :39)
+    fd = {}
+    for m in re.finditer(r"n=(\d+) half=False deals_simulated=(\d+) \(expected \d+\) cycling_found=(\d+) a\(n\)=(\d+) "
+                         r"longest_finite=(\d+)", long_runs):
+        fd[int(m.group(1))] = {"deals": int(m.group(2)), "cyc": int(m.group(3)), "longest": int(m.group(5))}
+    g["floyd_deals"] = fd
 
     # n = 14, 15 long deal runs with histograms (long_runs.txt:13-17)
     lr = {}

@@ -94,9 +94,10 @@ def test_tunes_agree(wl, oracle, tune):
         same(wl, oracle, wl.enumerate_job(job, wl.make_tune(**tune)), want)
 
 
-@pytest.mark.parametrize("mode,n", [(0, 10), (0, 11), (1, 10)])
-def test_floyd_sample_cross_check(wl, oracle, mode, n):
-    job = wl.make_job(n, mode, flags=wl.F_SAMPLE, sample_ppm=10000, seed=2024)
+@pytest.mark.parametrize("mode,n,ppm", [(0, 10, 10000), (0, 11, 10000), (1, 10, 10000), (0, 10, 1000000),
+                                         (1, 10, 1000000), (0, 9, 1000000)])
+def test_floyd_sample_cross_check(wl, oracle, mode, n, ppm):
+    job = wl.make_job(n, mode, flags=wl.F_SAMPLE, sample_ppm=ppm, seed=2024)
     f = wl.floyd_sample(job)
     b = wl.enumerate_job(job)
     o = oracle.floyd_sample_job(ojob(oracle, job))
@@ -146,6 +147,30 @@ def test_n14_canon_full(wl, golden):
     assert (f.s_count, f.s_cyc, f.s_lamsum, f.s_lensum, f.s_maxfin) == \
         (r["s_count"], r["s_cyc"], r["s_lamsum"], r["s_lensum"], r["s_maxfin"])
     assert 0.009 * g["positions"] < r["s_count"] < 0.011 * g["positions"]
+
+
+def floyd_key(r):
+    return (r.s_count, r.s_cyc, r.s_lamsum, r.s_lensum, r.s_maxfin)
+
+
+def test_floyd_full_range_a13(wl, golden):
+    """Every one of the 13! deals played with Floyd (sample rate 100%: the full-range cross-check of
+    gpu/war_gpu_floyd.py, recorded at data/long_runs.txt:35), by its own lexicographic enumeration: the recorded
+    a(13) and longest game, and every aggregate equal to Brent's on the same job (refill kernel, path memo)."""
+    job = wl.make_job(13, flags=wl.F_SAMPLE, sample_ppm=1000000, seed=1)
+    f = wl.floyd_sample(job)
+    g = golden["floyd_deals"][13]
+    assert (f.s_count, f.s_cyc, f.s_maxfin) == (g["deals"], g["cyc"], g["longest"])
+    assert floyd_key(f) == floyd_key(wl.enumerate_job(job))
+
+
+def test_floyd_full_range_canon13(wl, golden):
+    """The 5,748,019,200 canonical positions of n = 13 with Floyd (data/long_runs.txt:36) against Brent."""
+    job = wl.make_job(13, wl.CANON, flags=wl.F_SAMPLE, sample_ppm=1000000, seed=1)
+    f = wl.floyd_sample(job)
+    g = golden["canon_rule0"][13]
+    assert (f.s_count, f.s_cyc, f.s_maxfin) == (g["positions"], g["cycling"], g["longest"])
+    assert floyd_key(f) == floyd_key(wl.enumerate_job(job))
 
 
 def test_native_autotune_keeps_counts(wl, oracle):

@@ -33,7 +33,7 @@ def same(wl, a, b, with_turns=False):
         assert da[k] == db[k], k
 
 
-def test_each_job_same_alone_and_in_the_mix(wl):
+def test_each_job_same_alone_and_in_the_mix(wl, oracle):
     import serve
     jobs = mix(wl)
     alone = [wl.enumerate_job(j) for j in jobs]
@@ -41,25 +41,60 @@ def test_each_job_same_alone_and_in_the_mix(wl):
         ids = [s.submit(j) for j in jobs]
         got = s.wait_all(ids)
         st = s.stats()
+        mi = s.memo_info()
     for j, a, (r, info) in zip(jobs, alone, got):
         same(wl, r, a)
         assert info["finish_ms"] >= info["admit_ms"] >= info["submit_ms"]
     for j, a in zip(jobs, alone):
         if j.hi > j.lo and j.n > 1:
             same(wl, wl.enumerate_plain(j), a)
+    # the small jobs of the mix against the oracle as well
+    for j, (r, _) in zip(jobs, got):
+        if j.n <= 11:
+            want = oracle.to_dict(oracle.enumerate_job(oracle.make_job(j.n, j.mode, j.rule, j.flags, j.lo, j.hi,
+                                                                       j.hbins, j.dbins, j.blk)))
+            g = wl.to_dict(r)
+            for k in ("cyc", "done", "maxfin", "oncycle", "distinct_min", "shape_nonstd", "hist", "dhist", "endhist"):
+                assert g[k] == want[k], (j.n, j.mode, k)
     assert st["jobs_done"] == len(jobs)
     assert st["ticks"] >= 1
+    # the memo tables came from the arena reserved at create, inside it
+    assert mi["arena_bytes"] > 0 and 0 < mi["used_bytes"] <= mi["arena_bytes"] and mi["classes"] >= 2
 
 
 def test_admission_by_memory_budget(wl):
+    """A budget of three accumulator slots admits three jobs at a time and leaves nothing for a memo arena:
+    the jobs run without the memo, with the same results (including an n = 13 slice, whose class would
+    otherwise take a 2 GiB table)."""
     import serve
     jobs = [wl.make_job(11, lo=i * 1_000_000, hi=(i + 1) * 1_000_000, hbins=32) for i in range(12)]
+    jobs.append(wl.make_job(13, lo=2_000_000_000, hi=2_030_000_000, hbins=128))
     alone = [wl.enumerate_job(j) for j in jobs]
     with serve.Server(mem_budget=3 * serve.SIZEOF_DEVACC + 100) as s:
         ids = [s.submit(j) for j in jobs]
         got = s.wait_all(ids)
         st = s.stats()
+        mi = s.memo_info()
     assert st["peak_resident"] <= 3
+    assert mi == {"arena_bytes": 0, "used_bytes": 0, "classes": 0}
+    for j, a, (r, _) in zip(jobs, alone, got):
+        same(wl, r, a)
+        same(wl, wl.enumerate_plain(j), r)
+
+
+def test_memo_arena_inside_the_budget(wl):
+    """A budget with room for the slots and a small arena: the first class takes what fits, a later class
+    whose table no longer fits runs without one; every result is the same."""
+    import serve
+    jobs = [wl.make_job(13, lo=10 ** 9, hi=10 ** 9 + 2 * 10 ** 7, hbins=128),
+            wl.make_job(14, lo=5 * 10 ** 9, hi=5 * 10 ** 9 + 10 ** 7, hbins=128),
+            wl.make_job(13, lo=4 * 10 ** 9, hi=4 * 10 ** 9 + 10 ** 7, rule=1, hbins=64)]
+    alone = [wl.enumerate_job(j) for j in jobs]
+    budget = 8 * serve.SIZEOF_DEVACC + (8 << 20)          # 8 slots and an 8 MiB arena
+    with serve.Server(max_jobs=8, mem_budget=budget) as s:
+        got = s.wait_all([s.submit(j) for j in jobs])
+        mi = s.memo_info()
+    assert mi["arena_bytes"] == 8 << 20 and mi["used_bytes"] == 8 << 20 and mi["classes"] == 1
     for a, (r, _) in zip(alone, got):
         same(wl, r, a)
 
@@ -70,7 +105,8 @@ def test_poisson_stream_small(wl):
     with serve.Server() as s:
         results, lat, wall = serve.serve_stream(stream, s)
     assert all(r is not None for r in results)
-    assert serve.verify(stream[:40], results[:40]) == 0
+    assert serve.verify(stream[:60], results[:60]) == 0
+    assert any(j.rule for _, j in stream[:60]) and any(j.flags & wl.F_DISTINCT for _, j in stream[:60])
     assert serve.percentile(lat, 50) <= serve.percentile(lat, 99)
 
 

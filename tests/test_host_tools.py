@@ -21,6 +21,12 @@ def test_poisson_stream_is_seeded_and_in_range():
         assert j.hi - j.lo <= 10 ** 9 and (j.hi - j.lo >= 10 ** 4 or j.hi - j.lo == total)
         deals += j.mode == warlib.DEALS
     assert 0.65 < deals / len(a) < 0.75                                # 70% deals
+    rule1 = sum(j.rule for _, j in a) / len(a)
+    assert 0.15 < rule1 < 0.25                                         # 20% loser-first
+    canon = [j for _, j in a if j.mode == warlib.CANON]
+    dist = [j for j in canon if j.flags & warlib.F_DISTINCT]
+    assert 0.4 < len(dist) / len(canon) < 0.6 and all(j.dbins == 256 for j in dist)   # half of them --distinct
+    assert all(j.flags == 0 and j.dbins == 0 for _, j in a if j.mode == warlib.DEALS)
 
 
 def test_percentile():

@@ -136,3 +136,24 @@ def test_war17_resume(monkeypatch, oracle, tmp_path):
     calls.append(None)   # no more interruptions
     r = war17.run(9, per=4, batch_threads=256, out=out, resume=True)
     assert r[:3] == (218680, 362880, 28)
+
+
+def test_progress_file_schema_is_the_reference_one(monkeypatch, oracle, tmp_path):
+    """The drop-in writes its progress file with exactly the keys of gpu/war_gpu.py:331-338, in the same order
+    and with the same value types, as the reference's own files (tests/golden/progress_*_ref.json)."""
+    import os
+    import war_gpu
+    fake_engine(monkeypatch, oracle)
+    golden_dir = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    for name, kw in (("progress_deals13_ref.json", dict(hbins=64)),
+                     ("progress_canon13_ref.json", dict(canon=True, shape=True, dbins=4096))):
+        with open(os.path.join(golden_dir, name)) as f:
+            ref = json.load(f)
+        out = str(tmp_path / name)
+        war_gpu.run(8, out=out, quiet=True, **kw)
+        with open(out + ".progress") as f:
+            ours = json.load(f)
+        assert list(ours) == list(ref)
+        for k in ref:
+            assert type(ours[k]) is type(ref[k]), k
+        assert ours["next_start"] == ours["total"] and ours["n"] == 8
