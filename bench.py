@@ -446,7 +446,8 @@ def main():
         h2d = 0
         for a, b in spans:
             h2d += 24 * len(warlib.plan(warlib.make_job(n, mode, 0, w["flags"], a, b), tune.block_m if tune else 6)[2])
-        d2h = 73880 * len(spans)
+        import serve
+        d2h = serve.SIZEOF_DEVACC * len(spans)
         e2e = {"value": total / e2e_s, "unit": "positions/s" if mode else "deals/s", "h2d_bytes_per_step": h2d,
                "d2h_bytes_per_step": d2h, "api": "war_gpu.run" if ws == 1 else "warlib.enumerate_job",
                "check": "result tuple equal to the recorded one" if ws == 1 and "lo" not in w else None}

@@ -106,6 +106,7 @@ void merge_acc(const DevAcc& h, war_result* r, int hbins, int dbins) {
     if (h.s_maxfin > r->s_maxfin) r->s_maxfin = h.s_maxfin;
     r->units += h.units;
     r->memo_lookups += h.memo_lookups; r->memo_hits += h.memo_hits; r->memo_stores += h.memo_stores;
+    r->undetermined += h.undetermined;
     for (int i = 0; i < hbins; i++) r->hist[i] += h.hist[i];
     for (int i = 0; i < dbins; i++) r->dhist[i] += h.dhist[i];
     for (int i = 0; i < WAR_EBINS; i++) r->endhist[i] += h.endhist[i];

@@ -196,6 +196,7 @@ struct DevAcc {
     u64 memo_lookups, memo_hits, memo_stores;
     u64 work_next;   // persistent kernel: next work unit
     u64 status;      // nonzero: a game hit the turn cap
+    u64 undetermined;   // 5-bit engine: games undecided at the step cap (counted, not an error)
     u64 hist[WAR_HBINS_MAX];
     u64 dhist[WAR_DBINS_MAX];
     u64 endhist[WAR_EBINS];

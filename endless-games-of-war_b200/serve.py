@@ -25,7 +25,7 @@ import time
 sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
 import warlib  # noqa: E402
 
-SIZEOF_DEVACC = 19 * 8 + (warlib.WAR_HBINS_MAX + warlib.WAR_DBINS_MAX + warlib.WAR_EBINS) * 8
+SIZEOF_DEVACC = 20 * 8 + (warlib.WAR_HBINS_MAX + warlib.WAR_DBINS_MAX + warlib.WAR_EBINS) * 8
 
 
 class Server:

@@ -48,7 +48,7 @@ class Result(ctypes.Structure):
                 ("s_cyc", ctypes.c_uint64), ("s_lamsum", ctypes.c_uint64),
                 ("s_lensum", ctypes.c_uint64), ("s_maxfin", ctypes.c_uint64),
                 ("units", ctypes.c_uint64), ("memo_lookups", ctypes.c_uint64), ("memo_hits", ctypes.c_uint64),
-                ("memo_stores", ctypes.c_uint64), ("kernel_ms", ctypes.c_double),
+                ("memo_stores", ctypes.c_uint64), ("undetermined", ctypes.c_uint64), ("kernel_ms", ctypes.c_double),
                 ("hbins", ctypes.c_int32), ("dbins", ctypes.c_int32), ("blk", ctypes.c_int32),
                 ("status", ctypes.c_int32),
                 ("hist", ctypes.c_uint64 * WAR_HBINS_MAX), ("dhist", ctypes.c_uint64 * WAR_DBINS_MAX),

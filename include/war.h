@@ -113,6 +113,7 @@ typedef struct war_result {
     uint64_t s_count, s_cyc, s_lamsum, s_lensum, s_maxfin; /* sample aggregates (WAR_F_SAMPLE) */
     uint64_t units;          /* work units processed (diagnostic) */
     uint64_t memo_lookups, memo_hits, memo_stores; /* cycle memo traffic (war_tune.variant bit 2; diagnostic) */
+    uint64_t undetermined;   /* war_enumerate_wide: games still undecided at the step cap (gpu/war24.py:57, :98-103) */
     double kernel_ms;        /* device time of the enumeration kernel(s), CUDA events */
     int32_t hbins, dbins, blk, status;
     uint64_t hist[WAR_HBINS_MAX];

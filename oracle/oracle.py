@@ -3,6 +3,7 @@ bench.py's CPU-baseline leg use it as the checker; the product never imports it.
 
 * ``enumerate_job(job)``  -- liboracle.so (war_oracle.c), the C restatement of gpu/war_gpu.py.
 * ``floyd_sample_job(job)`` -- the same sample played with Floyd (gpu/war_gpu_floyd.py:95-105).
+* ``war24(job, det)``     -- the 5-bit program of gpu/war24.py (n <= 20, Floyd / streak test / Brent).
 * ``ref_war(n, rule)``    -- the reference's own cpu/war.cpp, compiled unmodified into oracle/_ref/
                              (result line format cpu/war.cpp:59), when that binary is present.
 * ``ref_distinct(n, t)``  -- cpu/distinct_cycles.c from oracle/_ref/ (output cpu/distinct_cycles.c:144-147).
@@ -38,7 +39,7 @@ class Result(ctypes.Structure):
                 ("s_cyc", ctypes.c_uint64), ("s_lamsum", ctypes.c_uint64),
                 ("s_lensum", ctypes.c_uint64), ("s_maxfin", ctypes.c_uint64),
                 ("units", ctypes.c_uint64), ("memo_lookups", ctypes.c_uint64), ("memo_hits", ctypes.c_uint64),
-                ("memo_stores", ctypes.c_uint64), ("kernel_ms", ctypes.c_double),
+                ("memo_stores", ctypes.c_uint64), ("undetermined", ctypes.c_uint64), ("kernel_ms", ctypes.c_double),
                 ("hbins", ctypes.c_int32), ("dbins", ctypes.c_int32), ("blk", ctypes.c_int32),
                 ("status", ctypes.c_int32),
                 ("hist", ctypes.c_uint64 * WAR_HBINS_MAX), ("dhist", ctypes.c_uint64 * WAR_DBINS_MAX),
@@ -59,6 +60,8 @@ def lib():
         _lib.oracle_enumerate.argtypes = [ctypes.POINTER(Job), ctypes.c_int, ctypes.POINTER(Result)]
         _lib.oracle_floyd_sample.argtypes = [ctypes.POINTER(Job), ctypes.c_int, ctypes.POINTER(Result)]
         _lib.oracle_enumerate_held.argtypes = [ctypes.POINTER(Job), ctypes.c_int, ctypes.POINTER(Result)]
+        _lib.oracle_war24.argtypes = [ctypes.POINTER(Job), ctypes.c_int, ctypes.c_uint32, ctypes.c_uint64, ctypes.c_int,
+                                      ctypes.POINTER(Result)]
         _lib.oracle_play_one.argtypes = [ctypes.c_uint64, ctypes.c_int, ctypes.c_uint64, ctypes.c_int,
                                          ctypes.c_int, ctypes.POINTER(ctypes.c_uint64),
                                          ctypes.POINTER(ctypes.c_uint64)]
@@ -105,6 +108,19 @@ def enumerate_held(job, threads=0):
     st = lib().oracle_enumerate_held(ctypes.byref(job), threads, ctypes.byref(r))
     if st != 0:
         raise ValueError("oracle_enumerate_held: status %d" % st)
+    return r
+
+
+DET_BRENT, DET_FLOYD, DET_STREAK = 0, 1, 2
+
+
+def war24(job, det=DET_STREAK, window=1, cap=0, threads=0):
+    """The 5-bit program of gpu/war24.py on ranks [lo, hi) of the n! deals (n <= 20): cyc, done, maxfin,
+    undetermined, turns (steps played) and, with Brent, the cycle-length histogram."""
+    r = Result()
+    st = lib().oracle_war24(ctypes.byref(job), det, window, cap, threads, ctypes.byref(r))
+    if st != 0:
+        raise ValueError("oracle_war24: status %d" % st)
     return r
 
 

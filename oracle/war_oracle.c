@@ -15,6 +15,7 @@
  *   loop_shape        Theorem-3 test      gpu/war_gpu.py:51-73
  *   floyd             second detector     gpu/war_gpu_floyd.py:95-105 (tortoise/hare, hare steps = game length)
  *   held-out card     n <= 17 deals       gpu/war17.py:36-113 (oracle_enumerate_held)
+ *   5-bit piles       n <= 20 deals       gpu/war24.py:31-140 (oracle_war24: Floyd, streak test, step cap)
  * Piles use the reference's layout: 4-bit cards in a uint64, top card in the low nibble, explicit
  * lengths.  Additions with no reference counterpart (turn totals, ending-length histogram, sample
  * aggregates) are computed from the same per-game results.
@@ -259,6 +260,7 @@ static void merge(war_result* dst, const war_result* src) {
     dst->s_count += src->s_count; dst->s_cyc += src->s_cyc; dst->s_lamsum += src->s_lamsum;
     dst->s_lensum += src->s_lensum;
     if (src->s_maxfin > dst->s_maxfin) dst->s_maxfin = src->s_maxfin;
+    dst->undetermined += src->undetermined;
     for (int i = 0; i < WAR_HBINS_MAX; i++) dst->hist[i] += src->hist[i];
     for (int i = 0; i < WAR_DBINS_MAX; i++) dst->dhist[i] += src->dhist[i];
     for (int i = 0; i < WAR_EBINS; i++) dst->endhist[i] += src->endhist[i];
@@ -470,6 +472,188 @@ int oracle_enumerate_held(const war_job* job, int nthreads, war_result* out) {
                     for (int l = i + 1, rr = n - 1; l < rr; l++, rr--) { t = a[l]; a[l] = a[rr]; a[rr] = t; }
                 }
             }
+        }
+    }
+    for (int t = 0; t < nthreads; t++) merge(out, &parts[t]);
+    free(parts);
+    return WAR_OK;
+}
+
+/* ---- the 5-bit program of gpu/war24.py: deals of n <= 20 cards ------------------------------------------
+ * Cards are 5 bits and a pile is two 64-bit words (lo, hi) with the top card in the lowest 5 bits and an
+ * explicit length (gpu/war24.py:31-47); a deal's rank is its lexicographic rank among the n! orders, unranked
+ * with the Lehmer code of :64-77 and stepped with the next permutation of :127-137.  Two detectors follow the
+ * reference line by line, each with its step cap (:57) after which a game counts as undetermined:
+ *   floyd   tortoise and hare, two hare turns per tortoise turn; cap tested after the tortoise turn (:82-95)
+ *   streak  odd n: anchor where the next winner holds an even number of cards, then expect the players to
+ *           alternate for lcm(n+1, W, L-1) turns and compare with the anchor (:96-125)
+ * and a third, Brent with the tortoise saved at turns W, 3W, 7W, ... (the engine's default), which is this
+ * repository's addition, like the loser-first rule (the reference plays rule 0 only).  The step count of an
+ * ending game is its length in every detector. */
+typedef struct { uint64_t lo, hi; } P5;
+typedef struct { P5 a, b; int la; } S5;
+enum { DET_BRENT = 0, DET_FLOYD = 1, DET_STREAK = 2 };
+
+static inline unsigned pop5(P5* p) {                        /* popc5, gpu/war24.py:31-35 */
+    unsigned c = (unsigned)(p->lo & 31u);
+    p->lo = (p->lo >> 5) | (p->hi << 59); p->hi >>= 5;
+    return c;
+}
+static inline void put5(P5* p, int L, uint64_t v, int bits) {   /* put, gpu/war24.py:36-41 */
+    int q = 5 * L;
+    uint64_t slo = (q < 64) ? (v << q) : 0ull;
+    uint64_t shi = (q >= 64) ? (v << (q - 64)) : ((q + bits > 64) ? (v >> (64 - q)) : 0ull);
+    p->lo |= slo; p->hi |= shi;
+}
+static inline int pstep5(S5* s, int n, int rule) {          /* pstep, gpu/war24.py:42-47 (+ rule 1) */
+    int lb = n - s->la;
+    unsigned ta = pop5(&s->a), tb = pop5(&s->b);
+    if (ta > tb) {
+        put5(&s->a, s->la - 1, rule ? ((uint64_t)tb | ((uint64_t)ta << 5)) : ((uint64_t)ta | ((uint64_t)tb << 5)), 10);
+        s->la += 1; return 1;
+    }
+    put5(&s->b, lb - 1, rule ? ((uint64_t)ta | ((uint64_t)tb << 5)) : ((uint64_t)tb | ((uint64_t)ta << 5)), 10);
+    s->la -= 1; return 0;
+}
+static inline int eq5(const S5* x, const S5* y) {
+    return x->a.lo == y->a.lo && x->a.hi == y->a.hi && x->b.lo == y->b.lo && x->b.hi == y->b.hi && x->la == y->la;
+}
+static int gcd5(int a, int b) { while (b) { int t = a % b; a = b; b = t; } return a; }
+static int lcm5(int a, int b) { return a / gcd5(a, b) * b; }
+
+/* Returns 0 = ends, 1 = cycles, 2 = undetermined; *steps = turns played (the game's length if it ends). */
+static int floyd5(S5 s, int n, int rule, uint64_t cap, uint64_t* steps_out) {      /* gpu/war24.py:82-95 */
+    S5 t = s, h = s;
+    uint64_t steps = 0;
+    for (;;) {
+        if (h.la == 0 || h.la == n) { *steps_out = steps; return 0; }
+        pstep5(&h, n, rule); steps++;
+        if (h.la == 0 || h.la == n) { *steps_out = steps; return 0; }
+        pstep5(&h, n, rule); steps++;
+        if (h.la == 0 || h.la == n) { *steps_out = steps; return 0; }
+        pstep5(&t, n, rule);
+        if (eq5(&t, &h)) { *steps_out = steps; return 1; }
+        if (steps > cap) { *steps_out = steps; return 2; }
+    }
+}
+
+static int streak5(S5 s, int n, int rule, uint64_t cap, uint64_t* steps_out) {      /* gpu/war24.py:96-125 */
+    int anch = 0, lam = 0, since = 0, prevw = -1;
+    S5 sv = s;
+    uint64_t steps = 0;
+    for (;;) {
+        if (s.la == 0 || s.la == n) { *steps_out = steps; return 0; }
+        if (steps > cap) { *steps_out = steps; return 2; }
+        if (!anch) {
+            unsigned ta = (unsigned)(s.a.lo & 31u), tb = (unsigned)(s.b.lo & 31u);
+            int ws = (ta > tb) ? s.la : (n - s.la), ls = n - ws;
+            if ((ws & 1) == 0 && ls >= 2) {
+                anch = 1; since = 0; prevw = -1;
+                lam = lcm5(n + 1, lcm5(ws, ls - 1));
+                sv = s;
+            }
+        }
+        int w = pstep5(&s, n, rule); steps++;
+        if (anch) {
+            if (w == prevw) anch = 0;
+            else {
+                prevw = w; since++;
+                if (since == lam) {
+                    if (eq5(&s, &sv)) { *steps_out = steps; return 1; }
+                    anch = 0;
+                }
+            }
+        }
+    }
+}
+
+static int brent5(S5 s, int n, int rule, uint64_t cap, uint64_t W, uint64_t* steps_out, uint64_t* lam_out) {
+    if (s.la == 0 || s.la == n) { *steps_out = 0; return 0; }
+    S5 t = s;
+    uint64_t rounds = 0, next = W, last = 0;
+    for (;;) {
+        pstep5(&s, n, rule); rounds++;
+        if (s.la == 0 || s.la == n) { *steps_out = rounds; return 0; }
+        if (eq5(&s, &t)) { *steps_out = rounds; *lam_out = rounds - last; return 1; }
+        if (rounds > cap) { *steps_out = rounds; return 2; }
+        if (rounds == next) { t = s; last = rounds; next = 2 * next + W; }
+    }
+}
+
+/* Ranks [lo, hi) of the n! deals of gpu/war24.py (2 <= n <= 20).  det: 0 Brent (first window `window`),
+ * 1 Floyd, 2 streak (odd n, rule 0).  cap: the step cap (0 = 2^22, gpu/war24.py:57).  Fills cyc, done,
+ * maxfin, undetermined, turns (steps played), endhist and, with Brent, the cycle-length histogram. */
+int oracle_war24(const war_job* job, int det, uint32_t window, uint64_t cap, int nthreads, war_result* out) {
+    if (!job || !out || job->n < 2 || job->n > 20 || job->mode != WAR_DEALS) return WAR_EINVAL;
+    if (det < 0 || det > 2 || (det == DET_STREAK && (!(job->n & 1) || job->rule))) return WAR_EINVAL;
+    if (job->hbins < 0 || job->hbins > WAR_HBINS_MAX || window < 1) return WAR_EINVAL;
+    const int n = job->n, rule = job->rule, hbins = det == DET_BRENT ? job->hbins : 0;
+    if (cap == 0) cap = 1ull << 22;
+    uint64_t f[21]; f[0] = 1;
+    for (int i = 1; i <= 20; i++) f[i] = f[i - 1] * (uint64_t)i;
+    if (job->lo > job->hi || job->hi > f[n]) return WAR_EINVAL;
+    memset(out, 0, sizeof(*out));
+    out->hbins = hbins;
+#ifdef _OPENMP
+    if (nthreads <= 0) nthreads = omp_get_max_threads();
+#else
+    nthreads = 1;
+#endif
+    uint64_t len = job->hi - job->lo;
+    if ((uint64_t)nthreads > len / 64 + 1) nthreads = (int)(len / 64 + 1);
+    war_result* parts = (war_result*)calloc((size_t)nthreads, sizeof(war_result));
+    if (!parts) return WAR_ENOMEM;
+    uint64_t pieces = (uint64_t)nthreads * 64u;
+    if (pieces > len) pieces = len ? len : 1;
+    #pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads)
+    for (long long pc = 0; pc < (long long)pieces; pc++) {
+        int tid = 0;
+#ifdef _OPENMP
+        tid = omp_get_thread_num();
+#endif
+        war_result* acc = &parts[tid];
+        uint64_t lo = job->lo + len * (uint64_t)pc / pieces, hi = job->lo + len * (uint64_t)(pc + 1) / pieces;
+        if (lo >= hi) continue;
+        unsigned char q[20];
+        {   /* Lehmer unrank of lo, gpu/war24.py:64-77 */
+            unsigned char avail[20];
+            for (int i = 0; i < n; i++) avail[i] = (unsigned char)i;
+            uint64_t r = lo;
+            int left = n;
+            for (int i = 0; i < n; i++) {
+                uint64_t fi = f[left - 1];
+                uint64_t d = left > 1 ? r / fi : 0;
+                if (left > 1) r %= fi;
+                q[i] = avail[d];
+                for (int k = (int)d; k < left - 1; k++) avail[k] = avail[k + 1];
+                left--;
+            }
+        }
+        for (uint64_t x = lo; x < hi; x++) {
+            S5 s;   /* the deal, gpu/war24.py:80-85: even positions to player 1, first card on top */
+            s.a.lo = s.a.hi = s.b.lo = s.b.hi = 0;
+            int la = 0, lb = 0;
+            for (int i = 0; i < n; i++) {
+                if ((i & 1) == 0) { put5(&s.a, la, q[i], 5); la++; }
+                else { put5(&s.b, lb, q[i], 5); lb++; }
+            }
+            s.la = la;
+            uint64_t steps = 0, lam = 0;
+            int res = det == DET_FLOYD ? floyd5(s, n, rule, cap, &steps)
+                    : det == DET_STREAK ? streak5(s, n, rule, cap, &steps)
+                    : brent5(s, n, rule, cap, window, &steps, &lam);
+            acc->done++;
+            acc->turns += steps;
+            if (res == 1) {
+                acc->cyc++;
+                if (hbins) acc->hist[lam < (uint64_t)(hbins - 1) ? lam : (uint64_t)(hbins - 1)]++;
+            } else if (res == 2) {
+                acc->undetermined++;
+            } else {
+                if (steps > acc->maxfin) acc->maxfin = steps;
+                acc->endhist[steps < WAR_EBINS - 1 ? steps : WAR_EBINS - 1]++;
+            }
+            if (x + 1 < hi) next_perm(q, n);   /* gpu/war24.py:127-137 */
         }
     }
     for (int t = 0; t < nthreads; t++) merge(out, &parts[t]);
