@@ -50,6 +50,27 @@ void fill_fact(u64* f);
 int resolve_tune(const war_job* job, const war_tune* in, Tune& t);
 int floyd_sample_run(const war_job* job, war_result* out);
 
+// Zeroes the device accumulators, runs `launch`, copies them back into c.h_acc.  Times the launch
+// with events on the launching stream.
+template <typename F>
+inline int run_launch(F launch, double* ms) {
+    Ctx& c = ctx();
+    cudaStream_t st = cur_stream();
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(c.d_acc, 0, sizeof(DevAcc), st)) != cudaSuccess) return cuda_fail(e, "memset acc");
+    if ((e = cudaEventRecord(c.ev0, st)) != cudaSuccess) return cuda_fail(e, "event record");
+    if ((e = launch(st)) != cudaSuccess) return cuda_fail(e, "kernel launch");
+    if ((e = cudaEventRecord(c.ev1, st)) != cudaSuccess) return cuda_fail(e, "event record");
+    if ((e = cudaMemcpyAsync(c.h_acc, c.d_acc, sizeof(DevAcc), cudaMemcpyDeviceToHost, st)) != cudaSuccess)
+        return cuda_fail(e, "copy acc");
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return cuda_fail(e, "kernel execution");
+    float f = 0.f;
+    cudaEventElapsedTime(&f, c.ev0, c.ev1);
+    if (ms) *ms += f;
+    if (c.h_acc->status) return fail(WAR_ECAP, "%llu game(s) passed the turn cap", (unsigned long long)c.h_acc->status);
+    return WAR_OK;
+}
+
 cudaError_t launch_sample_scan(const FloydArgs& a, int threads, u64 nthreads, ulonglong2* buf, u64 cap, DevAcc* acc,
                                cudaStream_t st);
 cudaError_t launch_floyd_enum(const FloydArgs& a, int blocks, DevAcc* acc, cudaStream_t st);

@@ -66,6 +66,15 @@ class JobStatus(ctypes.Structure):
                 ("admit_ms", ctypes.c_double), ("finish_ms", ctypes.c_double)]
 
 
+class WideCfg(ctypes.Structure):
+    _fields_ = [("det", ctypes.c_int32), ("cap", ctypes.c_uint32), ("threads", ctypes.c_int32),
+                ("blocks_per_sm", ctypes.c_int32), ("block_m", ctypes.c_int32), ("window", ctypes.c_int32),
+                ("defer", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
+DET_BRENT, DET_FLOYD, DET_STREAK = 0, 1, 2
+
+
 class DeviceInfo(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int32), ("sm_count", ctypes.c_int32), ("cc_major", ctypes.c_int32),
                 ("cc_minor", ctypes.c_int32), ("clock_mhz", ctypes.c_int32), ("max_threads_per_sm", ctypes.c_int32),
@@ -87,6 +96,7 @@ SYMBOLS = {
     "war_enumerate_plain": (ctypes.c_int, [ctypes.POINTER(Job), ctypes.POINTER(Result)]),
     "war_enumerate": (ctypes.c_int, [ctypes.POINTER(Job), ctypes.POINTER(Tune), ctypes.POINTER(Result)]),
     "war_enumerate_held": (ctypes.c_int, [ctypes.POINTER(Job), ctypes.POINTER(Tune), ctypes.POINTER(Result)]),
+    "war_enumerate_wide": (ctypes.c_int, [ctypes.POINTER(Job), ctypes.POINTER(WideCfg), ctypes.POINTER(Result)]),
     "war_floyd_sample": (ctypes.c_int, [ctypes.POINTER(Job), ctypes.POINTER(Result)]),
     "war_enumerate_noalloc": (ctypes.c_int, [ctypes.POINTER(Job), ctypes.POINTER(Tune), ctypes.POINTER(Result)]),
     "war_autotune": (ctypes.c_int, [ctypes.POINTER(Job), ctypes.POINTER(Tune), ctypes.c_double, ctypes.c_int32,
@@ -176,6 +186,14 @@ def enumerate_held(job, tune=None):
     r = Result()
     check(lib().war_enumerate_held(ctypes.byref(job), ctypes.byref(tune) if tune is not None else None,
                                    ctypes.byref(r)), "war_enumerate_held")
+    return r
+
+
+def enumerate_wide(job, det=DET_BRENT, cap=0, threads=0, blocks_per_sm=0, block_m=0, window=0, defer=0):
+    """war_enumerate_wide: deals of up to 20 cards with the 5-bit-pile engine (gpu/war24.py)."""
+    r = Result()
+    cfg = WideCfg(det, cap, threads, blocks_per_sm, block_m, window, defer, 0)
+    check(lib().war_enumerate_wide(ctypes.byref(job), ctypes.byref(cfg), ctypes.byref(r)), "war_enumerate_wide")
     return r
 
 

@@ -210,6 +210,25 @@ typedef struct war_job_status {
  * threads then; NULL = defaults (no memo).  war_enumerate sends n = 17 deal jobs here. */
 int war_enumerate_held(const war_job* job, const war_tune* tune, war_result* out);
 
+/* The 5-bit-pile engine (gpu/war24.py): deals of 2..20 cards (deal ranks are 64-bit), cards of 5 bits in
+ * 128-bit piles.  det picks the cycle test: WAR_DET_BRENT (tortoise saved at turns W, 3W, 7W, ...; the only
+ * one that measures cycle lengths for job.hbins), WAR_DET_FLOYD (gpu/war24.py:82-95) or WAR_DET_STREAK (odd n
+ * and rule 0 only: the players alternate for lcm(n+1, W, L-1) turns from an anchor, gpu/war24.py:96-125).  A
+ * game still undecided after `cap` turns counts in war_result.undetermined instead of cyc or the ending
+ * counts (gpu/war24.py:57).  All zero fields take defaults. */
+enum war_det { WAR_DET_BRENT = 0, WAR_DET_FLOYD = 1, WAR_DET_STREAK = 2 };
+typedef struct war_wide_cfg {
+    int32_t det;           /* war_det */
+    uint32_t cap;          /* step cap in turns (1..2^30; 0 = 2^22, gpu/war24.py:57) */
+    int32_t threads, blocks_per_sm, block_m, window, defer;   /* as in war_tune (defer: turns between services) */
+    int32_t reserved;
+} war_wide_cfg;
+
+/* Deals [lo, hi) of job.n = 2..20 cards with the 5-bit-pile engine: cyc, done, maxfin, turns (turns played by
+ * the detector), undetermined, endhist and (Brent) hist.  Only rule and hbins of the job apply (flags must be
+ * 0 or WAR_F_MEMO_KEEP, which has no effect).  Replaces the launch loop of gpu/war24.py:150-180. */
+int war_enumerate_wide(const war_job* job, const war_wide_cfg* cfg, war_result* out);
+
 /* Coordinate descent over war_tune for the class of `job` (block_m, games, threads, blocks per SM, window,
  * defer, variant, memo_bits), timed by war_enumerate's kernel time on a slice of job's range from its
  * middle, sized to take about slice_ms (0 = 400 ms); starts from *start (NULL = the library defaults) and

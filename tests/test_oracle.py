@@ -155,3 +155,44 @@ def test_held_out_restatement_agrees(oracle, golden, rule):
         if rule == 0:
             g = golden["deals_rule0"][n]
             assert (b["cyc"], b["done"], b["maxfin"]) == (g["cyc"], g["deals"], g["longest"])
+
+
+def test_war24_restatement_against_recorded_lines(oracle, golden):
+    """The oracle's restatement of gpu/war24.py reproduces the recorded runs it can finish here
+    (data/checks.txt:73-78: n = 5, 7, 9, 11 with the streak test, n = 10 with Floyd)."""
+    seen = 0
+    for e in golden["war24"]:
+        if e["hi"] - e["lo"] > 5 * 10 ** 7:
+            continue
+        det = oracle.DET_STREAK if e["det"] == "streak" else oracle.DET_FLOYD
+        r = oracle.war24(oracle.make_job(e["n"], lo=e["lo"], hi=e["hi"]), det)
+        assert (r.done, r.cyc, r.maxfin, r.undetermined) == (e["deals"], e["cyc"], e["longest"], e["undetermined"])
+        seen += 1
+    assert seen == 5
+
+
+@pytest.mark.parametrize("rule", [0, 1])
+def test_war24_brent_equals_the_4bit_oracle(oracle, rule):
+    """5-bit piles with Brent's reference schedule play exactly the 4-bit oracle's games: the same turn totals,
+    cycle lengths and ending lengths; Floyd and the streak test (rule 0, odd n) agree on every count."""
+    for n in range(2, 11):
+        a = oracle.to_dict(oracle.war24(oracle.make_job(n, rule=rule, hbins=256), oracle.DET_BRENT, 1))
+        b = oracle.to_dict(oracle.enumerate_job(oracle.make_job(n, rule=rule, hbins=256)))
+        for k in ("cyc", "done", "maxfin", "turns", "hist", "endhist"):
+            assert a[k] == b[k], (n, k)
+        f = oracle.war24(oracle.make_job(n, rule=rule), oracle.DET_FLOYD)
+        assert (f.cyc, f.done, f.maxfin, f.undetermined) == (b["cyc"], b["done"], b["maxfin"], 0)
+        if n % 2 and not rule:
+            s = oracle.war24(oracle.make_job(n), oracle.DET_STREAK)
+            assert (s.cyc, s.done, s.maxfin, s.undetermined) == (b["cyc"], b["done"], b["maxfin"], 0)
+
+
+def test_war24_step_cap(oracle):
+    """Below the games' lengths the step cap turns undecided games into undetermined ones, and only those."""
+    job = oracle.make_job(9)
+    full = oracle.war24(job, oracle.DET_FLOYD)
+    for det in (oracle.DET_FLOYD, oracle.DET_STREAK, oracle.DET_BRENT):
+        r = oracle.war24(job, det, 1, 20)
+        assert r.undetermined > 0
+        assert r.cyc + r.undetermined + sum(r.endhist) == full.done
+        assert r.maxfin <= 22 and r.cyc <= full.cyc

@@ -157,3 +157,45 @@ def test_progress_file_schema_is_the_reference_one(monkeypatch, oracle, tmp_path
         for k in ref:
             assert type(ours[k]) is type(ref[k]), k
         assert ours["next_start"] == ours["total"] and ours["n"] == 8
+
+
+def test_war24_lines_and_checkpoint(monkeypatch, oracle, golden, tmp_path):
+    """`war24.py n --det streak` for n = 5, 7, 9, 11 and `--det floyd` for n = 10 print the recorded lines
+    (data/checks.txt:73-78) apart from the time, with the oracle's restatement of gpu/war24.py standing in for
+    the engine; an interrupted run resumes from its checkpoint (pos, cyc, max, deals, und) to the same line."""
+    import warlib
+    import war24
+    dets = {warlib.DET_BRENT: oracle.DET_BRENT, warlib.DET_FLOYD: oracle.DET_FLOYD, warlib.DET_STREAK: oracle.DET_STREAK}
+
+    def enum(job, det=0, **kw):
+        return oracle.war24(oracle.make_job(job.n, job.mode, job.rule, 0, job.lo, job.hi), dets[det])
+    monkeypatch.setattr(warlib, "enumerate_wide", enum)
+    tm = re.compile(r" time=[0-9.]+s")
+    for e in [e for e in golden["war24"] if e["hi"] - e["lo"] <= 5 * 10 ** 7]:
+        buf = io.StringIO()
+        with contextlib.redirect_stdout(buf):
+            war24.main([str(e["n"]), "--det", e["det"], "--dir", str(tmp_path)])
+        assert tm.sub("", buf.getvalue().strip()) == tm.sub("", e["line"])
+    # interrupted after two spans of 50,000 deals, then resumed
+    monkeypatch.setattr(war24, "SPAN", 50000)
+    monkeypatch.setattr(war24, "CKPT_EVERY_S", -1.0)             # a checkpoint after every span
+    calls = []
+
+    def enum_stop(job, det=0, **kw):
+        calls.append(job.lo)
+        if len(calls) == 3:
+            raise KeyboardInterrupt("interrupted by the test")
+        return enum(job, det)
+    monkeypatch.setattr(warlib, "enumerate_wide", enum_stop)
+    with pytest.raises(KeyboardInterrupt):
+        war24.main(["9", "--dir", str(tmp_path), "--tag", "_t"])
+    with open(tmp_path / "war24_n9_streak_0_362880_t.ckpt") as f:
+        st = json.load(f)
+    assert list(st) == ["pos", "cyc", "max", "deals", "und"] and st["pos"] == 100000 == st["deals"]
+    calls.append(None)
+    buf = io.StringIO()
+    with contextlib.redirect_stdout(buf):
+        war24.main(["9", "--dir", str(tmp_path), "--tag", "_t", "--resume"])
+    want = next(e for e in golden["war24"] if e["n"] == 9)
+    assert tm.sub("", buf.getvalue().strip()) == tm.sub("", want["line"])
+    assert calls[4] == 100000                                     # resumed at the checkpoint
