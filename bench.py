@@ -54,7 +54,22 @@ WORKLOADS = {
     # a 2e8-deal slice from the middle of the n = 13 space (profiling size)
     "deals13slice": dict(n=13, mode=0, hbins=256, flags=0, lo=3013510400, hi=3213510400,
                          label="n=13 deals, ranks [3013510400, 3213510400)"),
+    # the reference's recorded 17-card slice (data/long_runs.txt:61-64: war24.py 17 --start 10^14 --count 10^9)
+    # on the 5-bit engine with each cycle test, and on the held-out-card engine
+    "wide17": dict(n=17, mode=0, hbins=0, flags=0, lo=10 ** 14, hi=10 ** 14 + 10 ** 9, engine="wide", det=2,
+                   label="n=17 deals [1e14, 1e14+1e9), war24.py 17 --det streak (5-bit engine)"),
+    "wide17floyd": dict(n=17, mode=0, hbins=0, flags=0, lo=10 ** 14, hi=10 ** 14 + 10 ** 9, engine="wide", det=1,
+                        label="n=17 deals [1e14, 1e14+1e9), war24.py 17 --det floyd (5-bit engine)"),
+    "wide17brent": dict(n=17, mode=0, hbins=0, flags=0, lo=10 ** 14, hi=10 ** 14 + 10 ** 9, engine="wide", det=0,
+                        label="n=17 deals [1e14, 1e14+1e9), Brent (5-bit engine)"),
+    "held17": dict(n=17, mode=0, hbins=0, flags=0, lo=10 ** 14, hi=10 ** 14 + 10 ** 9, engine="held",
+                   label="n=17 deals [1e14, 1e14+1e9), war17.py engine (card n-1 held out)"),
 }
+# Algorithmic integer operations per turn of the other engines, counted from their source like K_OPS_PER_TURN:
+# the 5-bit turn on 128-bit piles (two 128-bit pops 8, cards and compare 3, pair 3, position 2, the clamped
+# 128-bit shift of the pair 12, the masked XOR into four words 9, length 2: 39) plus Brent's four-word test and
+# bookkeeping (13) and the end test (2); the held-out turn is counted like the 4-bit turn.
+K_OPS_PER_TURN_ENGINE = {"refill": K_OPS_PER_TURN, "wide": 54, "held": K_OPS_PER_TURN}
 
 
 def measured_hbm_peak():
@@ -242,6 +257,24 @@ def cpu_baseline(w, target_s=12.0):
                           slice_len, "canonical-position" if mode else "deal", target_s)}
 
 
+def deal_extra_units(lo, hi, m):
+    """How many extra work units the engines copy to the device for deals [lo, hi): the aligned blocks of j!
+    ranks (j <= m) that cover the ragged ends around the main units of m! ranks (war_plan)."""
+    f = math.factorial
+
+    def blocks(x, y):
+        k = 0
+        while x < y:
+            j = m
+            while j > 0 and (x % f(j) or x + f(j) > y):
+                j -= 1
+            x += f(j)
+            k += 1
+        return k
+    a2, b2 = -(-lo // f(m)) * f(m), hi // f(m) * f(m)
+    return blocks(lo, a2) + blocks(b2, hi) if a2 < b2 else blocks(lo, hi)
+
+
 def peaks(warlib, table_bits, clk_mhz=None):
     """The measured ceilings on this GPU: integer issue (LOP3+IMAD), the ALU pipe alone, random 8-byte and
     32-byte gathers from a table of 2^table_bits words, and the nominal issue rate (SMs x 4 schedulers x 32
@@ -369,7 +402,13 @@ def main():
 
     floyd_ms = []
 
+    engine = w.get("engine", "refill")
+
     def step():
+        if engine == "wide":
+            return warlib.enumerate_wide(job, w["det"])
+        if engine == "held":
+            return warlib.enumerate_held(job)
         r = warlib.enumerate_job(job, tune)
         if w["flags"] & 8:
             f = warlib.floyd_sample(job)
@@ -406,6 +445,12 @@ def main():
             acc = [d["cyc"], d["done"], d["maxfin"], d["turns"], d["distinct_min"], d["oncycle"]]
         if "lo" not in w:
             check = verify(w, acc, r if ws == 1 else None, golden)
+        elif engine in ("wide", "held") and ws == 1:
+            rec = [e for e in golden["war24"] if (e["n"], e["lo"], e["hi"]) == (n, lo0, hi0)]
+            if not rec or (r.cyc, r.done, r.maxfin, r.undetermined) != (rec[0]["cyc"], rec[0]["deals"],
+                                                                        rec[0]["longest"], rec[0]["undetermined"]):
+                raise SystemExit("RESULT MISMATCH: %r" % ((r.cyc, r.done, r.maxfin, r.undetermined),))
+            check = "bit-exact vs the recorded war24.py run (data/long_runs.txt:63-64)"
 
     # e2e through the public drop-in API (war_gpu.run), host structs in, host results out, every copy inside
     # the timed region; its result is checked against the recorded one
@@ -415,7 +460,9 @@ def main():
         warlib.set_stream(0)
 
         def e2e_step():
-            if ws == 1 and "lo" not in w:
+            if engine != "refill":
+                step()
+            elif ws == 1 and "lo" not in w:
                 out = war_gpu.run(n, **kw)
                 dmin = sum(v // k for k, v in out[6].items()) if out[6] else None
                 verify(w, [out[0], out[1], out[2], None, dmin, None], None, golden)
@@ -445,7 +492,10 @@ def main():
             spans = [(lo, hi)]
         h2d = 0
         for a, b in spans:
-            h2d += 24 * len(warlib.plan(warlib.make_job(n, mode, 0, w["flags"], a, b), tune.block_m if tune else 6)[2])
+            if mode == 0:
+                h2d += 24 * deal_extra_units(a, b, min(n, tune.block_m if tune else 6))
+            else:
+                h2d += 24 * len(warlib.plan(warlib.make_job(n, mode, 0, w["flags"], a, b), tune.block_m)[2])
         import serve
         d2h = serve.SIZEOF_DEVACC * len(spans)
         e2e = {"value": total / e2e_s, "unit": "positions/s" if mode else "deals/s", "h2d_bytes_per_step": h2d,
@@ -456,7 +506,7 @@ def main():
     # once, outside the timed region: the batched-versus-plain ratio
     plain = None
     warlib.set_stream(stream.cuda_stream)
-    if not args.no_plain and ws == 1:
+    if not args.no_plain and ws == 1 and engine == "refill":
         rp = warlib.enumerate_plain(job)
         assert (rp.cyc, rp.done, rp.maxfin) == (res.cyc, res.done, res.maxfin), "plain and refill kernels disagree"
         plain = {"value": (hi - lo) / (rp.kernel_ms * 1e-3), "kernel_ms": rp.kernel_ms, "turns": rp.turns,
@@ -474,7 +524,8 @@ def main():
         pk = peaks(warlib, (tune.memo_bits or 24) if tune is not None and (tune.variant & 4) else 30,
                    clk_mhz=cs["sm_mhz"])
         issue_peak, alu_peak, nominal = pk["int_issue_ops_per_s"], pk["alu_ops_per_s"], pk["nominal_issue_ops_per_s"]
-        achieved = turns * K_OPS_PER_TURN / (kernel_ms * 1e-3)    # algorithmic int ops/s of the refill kernel
+        kops = K_OPS_PER_TURN_ENGINE[engine]
+        achieved = turns * kops / (kernel_ms * 1e-3)    # algorithmic int ops/s of the enumeration kernel
         memo = None
         if tune is not None and (tune.variant & 4) and res.memo_lookups:
             # the cycle memo's own traffic: one 8-byte word read per lookup, one written per store
@@ -510,7 +561,7 @@ def main():
                          "unit": "Tops/s (INT32 thread-ops)", "frac": achieved / issue_peak,
                          "peak_nominal": nominal / 1e12, "frac_of_nominal": achieved / nominal,
                          "alu_pipe_peak": alu_peak / 1e12, "frac_of_alu_pipe": achieved / alu_peak,
-                         "ops_per_turn": K_OPS_PER_TURN, "turns_per_launch": turns / max(1, launches // args.steps),
+                         "ops_per_turn": kops, "turns_per_launch": turns / max(1, launches // args.steps),
                          "traffic": (MEMO_DRAM_BYTES_PER_DEAL * total / max(1, launches // args.steps)
                                      if memo and mode == 0 and n == 13 else None),
                          "traffic_unit": "DRAM bytes per launch (ncu capture scaled by deals per launch)",
