@@ -541,6 +541,30 @@ def main():
                     "dram_bytes_per_deal": MEMO_DRAM_BYTES_PER_DEAL if mode == 0 and n == 13 else None,
                     "algorithmic_GBps": mbytes / (kernel_ms * 1e-3) / 1e9, "hbm_peak_GBps": hbm_peak,
                     "frac_of_hbm": mbytes / (kernel_ms * 1e-3) / 1e9 / hbm_peak, "hbm_peak_source": hbm_src}
+        # The integer-issue roofline of the turns (north-star's report: turns x ops per turn against the measured
+        # LOP3+IMAD ceiling and the nominal issue rate) and, for the memo kernel, the roofline that binds it:
+        # random 8-byte table reads against the measured random-gather ceiling of this GPU.
+        int_issue = {"achieved": achieved / 1e12, "peak": issue_peak / 1e12, "unit": "Tops/s (INT32 thread-ops)",
+                     "frac": achieved / issue_peak, "peak_nominal": nominal / 1e12, "frac_of_nominal": achieved / nominal,
+                     "alu_pipe_peak": alu_peak / 1e12, "frac_of_alu_pipe": achieved / alu_peak, "ops_per_turn": kops,
+                     "turns_per_launch": turns / max(1, launches // args.steps),
+                     "peak_source": "war_measure_int_peak on this GPU (LOP3+IMAD issue ceiling, measured); "
+                                    "nominal = SMs x 4 x 32 x median SM clock"}
+        per_launch = total / max(1, launches // args.steps)
+        if memo:
+            roofline = {"bound": "hbm_random_access", "achieved": memo["lookups_per_s"] / 1e9,
+                        "peak": memo["gather_peak_lookups_per_s"] / 1e9, "unit": "G lookups/s (random 8-byte reads)",
+                        "frac": memo["frac_of_gather_peak"],
+                        "traffic": (MEMO_DRAM_BYTES_PER_DEAL * per_launch if mode == 0 and n == 13 else None),
+                        "traffic_unit": "DRAM bytes per launch (ncu capture scaled by deals per launch)",
+                        "algorithmic_bytes_per_launch": 8.0 * (res.memo_lookups + res.memo_stores) / max(
+                            1, launches // args.steps),
+                        "peak_source": "war_measure_gather_peak on this GPU (random ld.global.cg of 8 bytes from a "
+                                       "table of the memo's size, measured)",
+                        "int_issue": int_issue}
+        else:
+            roofline = dict(int_issue, bound="int_issue", traffic=None,
+                            traffic_unit="DRAM bytes per launch: accumulators only (no table)")
         unit = "positions/s" if mode else "deals/s"
         value = total * args.steps / (ms_max * 1e-3)
         step_s = ms_max * 1e-3 / args.steps
@@ -557,16 +581,7 @@ def main():
             "kernel_ms": kernel_ms,
             "floyd_check_ms": (sum(floyd_ms[-args.steps:]) / args.steps) if floyd_ms else None,
             "gpu_launches": launches,
-            "roofline": {"bound": "int_issue", "achieved": achieved / 1e12, "peak": issue_peak / 1e12,
-                         "unit": "Tops/s (INT32 thread-ops)", "frac": achieved / issue_peak,
-                         "peak_nominal": nominal / 1e12, "frac_of_nominal": achieved / nominal,
-                         "alu_pipe_peak": alu_peak / 1e12, "frac_of_alu_pipe": achieved / alu_peak,
-                         "ops_per_turn": kops, "turns_per_launch": turns / max(1, launches // args.steps),
-                         "traffic": (MEMO_DRAM_BYTES_PER_DEAL * total / max(1, launches // args.steps)
-                                     if memo and mode == 0 and n == 13 else None),
-                         "traffic_unit": "DRAM bytes per launch (ncu capture scaled by deals per launch)",
-                         "peak_source": "war_measure_int_peak on this GPU (LOP3+IMAD issue ceiling, measured); "
-                                        "nominal = SMs x 4 x 32 x median SM clock"},
+            "roofline": roofline,
             "peaks": pk,
             "clocks": cs,
             "check": check,

@@ -47,17 +47,29 @@ DEFAULT = {"block_m": 5, "games": 2, "threads": 512, "blocks_per_sm": 0, "window
            "memo_bits": 24}
 
 
+_device_name = None
+_cache = {"mtime": None, "data": {}}
+
+
 def key(n, mode, rule, flags, device=None):
+    global _device_name
     if device is None:
-        device = warlib.device_info().name.decode()
+        if _device_name is None:      # the device's properties once per process (the query takes milliseconds)
+            _device_name = warlib.device_info().name.decode()
+        device = _device_name
     return "%s|n=%d|mode=%d|rule=%d|flags=%d" % (device, n, mode, rule, flags & ~(warlib.F_SAMPLE | warlib.F_MEMO_KEEP))
 
 
 def load_cache():
-    if os.path.exists(CACHE):
+    """The stored tunes, re-read only when the file changed."""
+    if not os.path.exists(CACHE):
+        return {}
+    m = os.path.getmtime(CACHE)
+    if _cache["mtime"] != m:
         with open(CACHE) as f:
-            return json.load(f)
-    return {}
+            _cache["data"] = json.load(f)
+        _cache["mtime"] = m
+    return _cache["data"]
 
 
 def default_tune(n, mode, rule, flags):
