@@ -21,8 +21,8 @@
 //   the two words plus their sentinels.
 // * Detectors (template DET), each with the step cap after which a game counts as undetermined:
 //   Brent with the tortoise saved at turns W, 3W, 7W, ... (the default; its cycle length feeds the
-//   histogram), Floyd's tortoise and hare (gpu/war24.py:82-95), and the streak test for odd n
-//   (gpu/war24.py:96-125): anchor where the next winner holds an even number of cards, then expect the
+//   histogram), Floyd's tortoise and hare (gpu/war24.py:85-97), and the streak test for odd n
+//   (gpu/war24.py:98-125): anchor where the next winner holds an even number of cards, then expect the
 //   players to alternate for lcm(n+1, W, L-1) turns and compare with the anchor.  Every detector gives the
 //   same counts whenever nothing reaches the cap; the step count of an ending game is its length.
 #include <algorithm>
@@ -106,7 +106,7 @@ __device__ __forceinline__ bool wide_fetch(WEnum& E, const WideArgs& a, u64* cou
         const Unit U = a.units[u - a.main_count];
         r = U.r; j = U.j;
     }
-    // lexicographic unrank (gpu/war24.py:64-77) straight into the split deck
+    // lexicographic unrank (gpu/war24.py:60-74) straight into the split deck
     const int n = a.n;
     u32 avail = (1u << n) - 1u;
     u64 A = 0, B = 0;
@@ -189,7 +189,7 @@ __global__ void __launch_bounds__(1024) wide_kernel(const __grid_constant__ Wide
         for (int k = 0; k < period; k++) {
             const bool open = kind == K_NONE;
             if (DET == DET_FLOYD) {
-                // two hare turns, one tortoise turn (gpu/war24.py:87-95)
+                // two hare turns, one tortoise turn (gpu/war24.py:88-96)
                 turn5<RULE>(a0, a1, b0, b1, la, n1);
                 const bool e1 = (la == 0u) | (la == n);
                 turn5<RULE>(a0, a1, b0, b1, la, n1);
@@ -201,7 +201,7 @@ __global__ void __launch_bounds__(1024) wide_kernel(const __grid_constant__ Wide
                 rounds = open ? r2 : rounds;
                 kind = open ? kk : kind;
             } else if (DET == DET_STREAK) {
-                // anchor where the next winner holds an even number of cards (gpu/war24.py:104-110)
+                // anchor where the next winner holds an even number of cards (gpu/war24.py:104-112)
                 if (!anch) {
                     const u32 ws = ((u32)a0 & 31u) > ((u32)b0 & 31u) ? la : n - la;
                     // (a lane whose game is decided keeps stepping it until the service, so its pile
@@ -211,7 +211,7 @@ __global__ void __launch_bounds__(1024) wide_kernel(const __grid_constant__ Wide
                 }
                 const u32 w = turn5<RULE>(a0, a1, b0, b1, la, n1) ? 1u : 0u;
                 bool cy = false;
-                if (anch) {   // the players must alternate for lam turns (gpu/war24.py:112-120)
+                if (anch) {   // the players must alternate for lam turns (gpu/war24.py:114-123)
                     if (w == prevw) anch = false;
                     else {
                         prevw = w;
@@ -353,7 +353,7 @@ extern "C" int war_enumerate_wide(const war_job* job, const war_wide_cfg* cfg, w
     for (int i = 1; i <= 20; i++) a.fact[i] = a.fact[i - 1] * (u64)i;
     a.n = job->n; a.m = block_m; a.rule = job->rule; a.hbins = hbins; a.W = W; a.defer = defer; a.cap = cap;
     a.units = cx.d_units;
-    for (int ws = 2; ws + 2 <= job->n; ws += 2) {   // gpu/war24.py:106-109: lcm(n+1, lcm(W, L-1))
+    for (int ws = 2; ws + 2 <= job->n; ws += 2) {   // gpu/war24.py:109: lcm(n+1, lcm(W, L-1))
         auto gcd = [](u64 x, u64 y) { while (y) { u64 t = x % y; x = y; y = t; } return x; };
         const u64 l1 = (u64)ws / gcd(ws, job->n - ws - 1) * (u64)(job->n - ws - 1);
         a.lamtab[ws] = (u32)((u64)(job->n + 1) / gcd(job->n + 1, l1) * l1);

@@ -1,7 +1,7 @@
 """Count the deals of single-suit War that never end, for up to 20 cards, on a B200.
 
 Drop-in for the reference's gpu/war24.py: the same command line, the same checkpoint and progress files, the
-same result line (gpu/war24.py:141-210).  The work runs in libwar.so's 5-bit-pile engine
+same result line (gpu/war24.py:158-210).  The work runs in libwar.so's 5-bit-pile engine
 (war_enumerate_wide: 5-bit cards in 128-bit piles, a persistent refill kernel) through ctypes.
 
 Rule (Spivey 2010): the higher top card wins; the winning card, then the losing card, go under the winner's
@@ -11,8 +11,8 @@ top).  Deal ranks are 64-bit, so n <= 20.
 Cycle detection:
   --det streak  (default; odd n only) the players alternate for lcm(n+1, W, L-1) turns after an anchor where
                 the next winner holds an even number of cards, and the state is compared with the anchor
-                (Spivey Thm 6) — gpu/war24.py:96-125.
-  --det floyd   tortoise and hare (any n) — gpu/war24.py:82-95.
+                (Spivey Thm 6) — gpu/war24.py:98-125.
+  --det floyd   tortoise and hare (any n) — gpu/war24.py:85-97.
   --det brent   Brent's cycle test (any n; this engine's fastest, not in the reference).
 Games still undecided after 2^22 turns are counted as undetermined.
 
@@ -41,7 +41,7 @@ CKPT_EVERY_S = 10.0
 
 
 def run(n, det="streak", lo=0, hi=None, resume=False, tag="", directory=None):
-    """Deals [lo, hi) of n cards (gpu/war24.py:150-200).  Returns (cycling, longest_finite, deals, undetermined,
+    """Deals [lo, hi) of n cards (gpu/war24.py:186-201).  Returns (cycling, longest_finite, deals, undetermined,
     elapsed_s).  Writes war24_<n>_<det>_<lo>_<hi><tag>.ckpt (JSON: pos, cyc, max, deals, und) and appends to
     the matching .progress log, as the reference does; resume=True continues from the checkpoint."""
     total_all = math.factorial(n)
@@ -83,7 +83,7 @@ def run(n, det="streak", lo=0, hi=None, resume=False, tag="", directory=None):
 
 
 def result_line(n, det, lo, hi, cyc, mx, deals, und, el):
-    """The result line of gpu/war24.py:203-205."""
+    """The result line of gpu/war24.py:204-205."""
     return (f"n={n} det={det} range=[{lo},{hi}) deals_simulated={deals} (expected {hi - lo}) "
             f"cycling={cyc} longest_finite={mx} undetermined={und} time={el:.1f}s")
 

@@ -113,7 +113,7 @@ typedef struct war_result {
     uint64_t s_count, s_cyc, s_lamsum, s_lensum, s_maxfin; /* sample aggregates (WAR_F_SAMPLE) */
     uint64_t units;          /* work units processed (diagnostic) */
     uint64_t memo_lookups, memo_hits, memo_stores; /* cycle memo traffic (war_tune.variant bit 2; diagnostic) */
-    uint64_t undetermined;   /* war_enumerate_wide: games still undecided at the step cap (gpu/war24.py:57, :98-103) */
+    uint64_t undetermined;   /* war_enumerate_wide: games still undecided at the step cap (gpu/war24.py:57, :103, :117) */
     double kernel_ms;        /* device time of the enumeration kernel(s), CUDA events */
     int32_t hbins, dbins, blk, status;
     uint64_t hist[WAR_HBINS_MAX];
@@ -212,8 +212,8 @@ int war_enumerate_held(const war_job* job, const war_tune* tune, war_result* out
 
 /* The 5-bit-pile engine (gpu/war24.py): deals of 2..20 cards (deal ranks are 64-bit), cards of 5 bits in
  * 128-bit piles.  det picks the cycle test: WAR_DET_BRENT (tortoise saved at turns W, 3W, 7W, ...; the only
- * one that measures cycle lengths for job.hbins), WAR_DET_FLOYD (gpu/war24.py:82-95) or WAR_DET_STREAK (odd n
- * and rule 0 only: the players alternate for lcm(n+1, W, L-1) turns from an anchor, gpu/war24.py:96-125).  A
+ * one that measures cycle lengths for job.hbins), WAR_DET_FLOYD (gpu/war24.py:85-97) or WAR_DET_STREAK (odd n
+ * and rule 0 only: the players alternate for lcm(n+1, W, L-1) turns from an anchor, gpu/war24.py:98-125).  A
  * game still undecided after `cap` turns counts in war_result.undetermined instead of cyc or the ending
  * counts (gpu/war24.py:57).  All zero fields take defaults. */
 enum war_det { WAR_DET_BRENT = 0, WAR_DET_FLOYD = 1, WAR_DET_STREAK = 2 };
@@ -226,7 +226,7 @@ typedef struct war_wide_cfg {
 
 /* Deals [lo, hi) of job.n = 2..20 cards with the 5-bit-pile engine: cyc, done, maxfin, turns (turns played by
  * the detector), undetermined, endhist and (Brent) hist.  Only rule and hbins of the job apply (flags must be
- * 0 or WAR_F_MEMO_KEEP, which has no effect).  Replaces the launch loop of gpu/war24.py:150-180. */
+ * 0 or WAR_F_MEMO_KEEP, which has no effect).  Replaces the launch loop of gpu/war24.py:186-201. */
 int war_enumerate_wide(const war_job* job, const war_wide_cfg* cfg, war_result* out);
 
 /* Coordinate descent over war_tune for the class of `job` (block_m, games, threads, blocks per SM, window,

@@ -15,7 +15,7 @@
  *   loop_shape        Theorem-3 test      gpu/war_gpu.py:51-73
  *   floyd             second detector     gpu/war_gpu_floyd.py:95-105 (tortoise/hare, hare steps = game length)
  *   held-out card     n <= 17 deals       gpu/war17.py:36-113 (oracle_enumerate_held)
- *   5-bit piles       n <= 20 deals       gpu/war24.py:31-140 (oracle_war24: Floyd, streak test, step cap)
+ *   5-bit piles       n <= 20 deals       gpu/war24.py:31-139 (oracle_war24: Floyd, streak test, step cap)
  * Piles use the reference's layout: 4-bit cards in a uint64, top card in the low nibble, explicit
  * lengths.  Additions with no reference counterpart (turn totals, ending-length histogram, sample
  * aggregates) are computed from the same per-game results.
@@ -522,7 +522,7 @@ static int gcd5(int a, int b) { while (b) { int t = a % b; a = b; b = t; } retur
 static int lcm5(int a, int b) { return a / gcd5(a, b) * b; }
 
 /* Returns 0 = ends, 1 = cycles, 2 = undetermined; *steps = turns played (the game's length if it ends). */
-static int floyd5(S5 s, int n, int rule, uint64_t cap, uint64_t* steps_out) {      /* gpu/war24.py:82-95 */
+static int floyd5(S5 s, int n, int rule, uint64_t cap, uint64_t* steps_out) {      /* gpu/war24.py:85-97 */
     S5 t = s, h = s;
     uint64_t steps = 0;
     for (;;) {
@@ -537,7 +537,7 @@ static int floyd5(S5 s, int n, int rule, uint64_t cap, uint64_t* steps_out) {   
     }
 }
 
-static int streak5(S5 s, int n, int rule, uint64_t cap, uint64_t* steps_out) {      /* gpu/war24.py:96-125 */
+static int streak5(S5 s, int n, int rule, uint64_t cap, uint64_t* steps_out) {      /* gpu/war24.py:98-125 */
     int anch = 0, lam = 0, since = 0, prevw = -1;
     S5 sv = s;
     uint64_t steps = 0;
@@ -615,7 +615,7 @@ int oracle_war24(const war_job* job, int det, uint32_t window, uint64_t cap, int
         uint64_t lo = job->lo + len * (uint64_t)pc / pieces, hi = job->lo + len * (uint64_t)(pc + 1) / pieces;
         if (lo >= hi) continue;
         unsigned char q[20];
-        {   /* Lehmer unrank of lo, gpu/war24.py:64-77 */
+        {   /* Lehmer unrank of lo, gpu/war24.py:60-74 */
             unsigned char avail[20];
             for (int i = 0; i < n; i++) avail[i] = (unsigned char)i;
             uint64_t r = lo;
@@ -630,7 +630,7 @@ int oracle_war24(const war_job* job, int det, uint32_t window, uint64_t cap, int
             }
         }
         for (uint64_t x = lo; x < hi; x++) {
-            S5 s;   /* the deal, gpu/war24.py:80-85: even positions to player 1, first card on top */
+            S5 s;   /* the deal, gpu/war24.py:76-82: even positions to player 1, first card on top */
             s.a.lo = s.a.hi = s.b.lo = s.b.hi = 0;
             int la = 0, lb = 0;
             for (int i = 0; i < n; i++) {
@@ -653,7 +653,7 @@ int oracle_war24(const war_job* job, int det, uint32_t window, uint64_t cap, int
                 if (steps > acc->maxfin) acc->maxfin = steps;
                 acc->endhist[steps < WAR_EBINS - 1 ? steps : WAR_EBINS - 1]++;
             }
-            if (x + 1 < hi) next_perm(q, n);   /* gpu/war24.py:127-137 */
+            if (x + 1 < hi) next_perm(q, n);   /* gpu/war24.py:129-139 */
         }
     }
     for (int t = 0; t < nthreads; t++) merge(out, &parts[t]);
