@@ -3,8 +3,10 @@
 For one (n, mode, rule, flag class) it times the kernel on a representative contiguous slice of the rank
 space (about `slice_s` seconds of work, taken from the middle of the space) and searches, one coordinate
 at a time, over
-    block_m        work-unit size: m! consecutive orders per unit        (4..7)
-    games          games in flight per thread                            (1, 2)
+    block_m        work-unit size: m! consecutive orders per unit        (4..8)
+    games          games in flight per thread                            (1, 2, 4)
+    chunk          units a lane takes from the work counter at a time: chunks of chunk x m! consecutive ranks
+                   (1 .. 1456: with m = 6 from 720 to 2^20 ranks)
     threads        block size                                            (128..1024)
     blocks_per_sm  resident blocks (0 = as many as fit)
     window         Brent's first tortoise window                         (8..128)
@@ -34,8 +36,9 @@ import warlib  # noqa: E402
 
 CACHE = os.path.join(HERE, "tune_cache.json")
 SPACE = {
-    "block_m": [4, 5, 6, 7],
-    "games": [1, 2],
+    "block_m": [4, 5, 6, 7, 8],
+    "games": [1, 2, 4],
+    "chunk": [1, 8, 64, 512, 1456],
     "threads": [128, 256, 512, 1024],
     "blocks_per_sm": [0, 1, 2, 3, 4],
     "window": [8, 16, 32, 64, 128],
@@ -44,7 +47,7 @@ SPACE = {
     "memo_bits": [26, 28, 29, 30],
 }
 DEFAULT = {"block_m": 5, "games": 2, "threads": 512, "blocks_per_sm": 0, "window": 32, "defer": 8, "variant": 1,
-           "memo_bits": 24}
+           "memo_bits": 24, "chunk": 1}
 
 
 _device_name = None
@@ -94,13 +97,15 @@ def cached_tune(n, mode, rule, flags):
     if not t:
         return None
     return warlib.make_tune(t["threads"], t["blocks_per_sm"], t["games"], t["block_m"], t["window"], t["defer"],
-                            t.get("variant", 0), t.get("memo_bits", 0))
+                            t.get("variant", 0), t.get("memo_bits", 0), t.get("chunk", 0))
 
 
 def _legal(n, mode, flags, cfg):
     if mode == warlib.CANON and (flags & warlib.F_DISTINCT) and cfg["window"] < 128:
         return False          # the free on-cycle test needs a first window at least as long as the cycles
     if cfg["games"] == 2 and cfg["threads"] > 512:
+        return False
+    if cfg["games"] == 4 and (cfg["threads"] > 256 or cfg["variant"] not in (3, 31)):
         return False
     return cfg["block_m"] <= (n - 1 if mode else n)
 
@@ -137,7 +142,7 @@ def measure(job, cfg, reps=2):
     return best, res
 
 
-def autotune(n, mode=warlib.DEALS, rule=0, flags=0, slice_s=0.4, passes=2, verbose=True):
+def autotune(n, mode=warlib.DEALS, rule=0, flags=0, slice_s=0.4, passes=2, verbose=True, dims=None):
     cur = dict(DEFAULT)
     if mode == warlib.CANON:
         cur.update(block_m=5, window=128 if flags & warlib.F_DISTINCT else 64)
@@ -153,6 +158,8 @@ def autotune(n, mode=warlib.DEALS, rule=0, flags=0, slice_s=0.4, passes=2, verbo
     for _ in range(passes):
         improved = False
         for name, values in SPACE.items():
+            if dims and name not in dims:
+                continue
             for v in values:
                 if v == cur[name]:
                     continue
@@ -194,10 +201,11 @@ def main():
     ap.add_argument("--slice-s", type=float, default=0.4)
     ap.add_argument("--full", action="store_true", help="time every configuration on the whole space")
     ap.add_argument("--passes", type=int, default=2)
+    ap.add_argument("--dims", default=None, help="comma-separated dimensions to search (default: all)")
     a = ap.parse_args()
     flags = (warlib.F_DISTINCT if a.distinct else 0) | (warlib.F_SHAPE if a.shape else 0)
     e = autotune(a.n, warlib.CANON if a.canon else warlib.DEALS, a.rule, flags, 1e9 if a.full else a.slice_s,
-                 a.passes)
+                 a.passes, dims=a.dims.split(",") if a.dims else None)
     print(json.dumps(e))
 
 

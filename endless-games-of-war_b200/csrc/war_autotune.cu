@@ -19,13 +19,14 @@ struct Dim {
 const std::vector<Dim>& dims() {
     static const std::vector<Dim> d = {
         {"block_m", &war_tune::block_m, {4, 5, 6, 7}},
-        {"games", &war_tune::games, {1, 2}},
+        {"games", &war_tune::games, {1, 2, 4}},
         {"threads", &war_tune::threads, {128, 256, 512, 1024}},
         {"blocks_per_sm", &war_tune::blocks_per_sm, {0, 1, 2, 3, 4}},
         {"window", &war_tune::window, {8, 16, 32, 64, 128}},
         {"defer", &war_tune::defer, {1, 2, 4, 8, 12, 16, 24, 32}},
         {"variant", &war_tune::variant, {0, 1, 2, 3, 6, 7, 14, 15, 30, 31}},
         {"memo_bits", &war_tune::memo_bits, {24, 26, 28, 30}},
+        {"chunk", &war_tune::chunk, {1, 8, 64, 512, 1456}},
     };
     return d;
 }
@@ -34,6 +35,7 @@ bool legal(const war_job& job, const war_tune& t) {
     const bool canon = job.mode == WAR_CANON;
     if (canon && (job.flags & WAR_F_DISTINCT) && t.window < 128) return false;   // the free on-cycle test
     if (t.games == 2 && t.threads > 512) return false;
+    if (t.games == 4 && (t.threads > 256 || (t.variant != 3 && t.variant != 31))) return false;
     return t.block_m <= (canon ? job.n - 1 : job.n);
 }
 

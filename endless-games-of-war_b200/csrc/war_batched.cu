@@ -5,7 +5,7 @@
 namespace war {
 
 template <int RULE, int G, bool CANON, bool SHAPE, bool EXTRA, int V>
-__global__ void __launch_bounds__(G == 1 ? 1024 : 512) batched_kernel(const __grid_constant__ BatchArgs a,
+__global__ void __launch_bounds__(G == 1 ? 1024 : (G == 2 ? 512 : 256)) batched_kernel(const __grid_constant__ BatchArgs a,
                                                                      DevAcc* __restrict__ acc) {
     extern __shared__ u32 sh[];
     refill_dispatch<RULE, G, CANON, SHAPE, EXTRA, V>(a, acc, &acc->work_next, sh);
@@ -25,6 +25,10 @@ static BatchedFn pick_g(int canon, int shape, int extra) {
 
 template <int V>
 static BatchedFn pick_v(int canon, int rule, int shape, int extra, int games) {
+    if (games == 4) {   // four games per lane: compiled for the product variants only (3: no memo, 31: path memo)
+        if constexpr (V == 3 || V == 31) return rule ? pick_g<1, 4, V>(canon, shape, extra) : pick_g<0, 4, V>(canon, shape, extra);
+        return nullptr;
+    }
     if (rule) return games == 2 ? pick_g<1, 2, V>(canon, shape, extra) : pick_g<1, 1, V>(canon, shape, extra);
     return games == 2 ? pick_g<0, 2, V>(canon, shape, extra) : pick_g<0, 1, V>(canon, shape, extra);
 }
@@ -53,6 +57,7 @@ cudaError_t launch_batched(const BatchArgs& a, int canon, int rule, int shape, c
                            cudaStream_t st) {
     int extra = (a.distinct || a.sample) ? 1 : 0;
     BatchedFn fn = pick(canon, rule, canon && shape, extra, bs.games, bs.variant);
+    if (!fn) return cudaErrorInvalidConfiguration;
     size_t shmem = sizeof(u32) * (size_t)(a.hbins + WAR_EBINS);
     fn<<<bs.blocks, bs.threads, shmem, st>>>(a, acc);
     note_launch();
@@ -62,6 +67,7 @@ cudaError_t launch_batched(const BatchArgs& a, int canon, int rule, int shape, c
 int batched_max_blocks_per_sm(int canon, int rule, int shape, int distinct, int sample, int threads, int games,
                               int hbins, int variant) {
     BatchedFn fn = pick(canon, rule, canon && shape, (distinct || sample) ? 1 : 0, games, variant);
+    if (!fn) return 0;   // a combination that is not compiled (four games per lane outside variants 3 and 31)
     int nb = 0;
     size_t shmem = sizeof(u32) * (size_t)(hbins + WAR_EBINS);
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, threads, shmem) != cudaSuccess) return 0;

@@ -183,8 +183,10 @@ int resolve_tune(const war_job* job, const war_tune* in, Tune& t) {
     t.defer = (in && in->defer) ? in->defer : 1;
     t.variant = in ? in->variant : 0;
     t.memo_bits = (in && in->memo_bits) ? in->memo_bits : 24;
+    t.chunk = (in && in->chunk) ? in->chunk : 1;
     if (t.threads < 64 || t.threads > 1024 || (t.threads & 31)) return fail(WAR_EINVAL, "tune.threads=%d", t.threads);
-    if (t.games != 1 && t.games != 2) return fail(WAR_EINVAL, "tune.games=%d (1 or 2)", t.games);
+    if (t.games != 1 && t.games != 2 && t.games != 4) return fail(WAR_EINVAL, "tune.games=%d (1, 2 or 4)", t.games);
+    if (t.chunk < 1 || t.chunk > 4096) return fail(WAR_EINVAL, "tune.chunk=%d (1..4096)", t.chunk);
     if (t.block_m < 1 || t.block_m > 8) return fail(WAR_EINVAL, "tune.block_m=%d (1..8)", t.block_m);
     if (t.window < 1 || t.window > (1 << 16) || (t.window & (t.window - 1))) return fail(WAR_EINVAL, "tune.window=%d", t.window);
     if (t.defer < 1 || t.defer > 32) return fail(WAR_EINVAL, "tune.defer=%d (1..32)", t.defer);
@@ -610,6 +612,7 @@ int war_enumerate(const war_job* job, const war_tune* tune, war_result* out) {
     a.seed = job->seed;
     a.thr = ((u64)job->sample_ppm << 32) / 1000000u;
     a.units = c.d_units;
+    a.chunk = (u32)t.chunk;
     if (t.variant & 4) {   // the cycle memo
         // its entry layout: the form the variant selects, and the shape-carrying values of a canonical scan
         // with the loop-shape test

@@ -33,7 +33,7 @@ struct Plan {
 };
 
 struct Tune {
-    int threads, blocks_per_sm, games, block_m, window, defer, variant, memo_bits;
+    int threads, blocks_per_sm, games, block_m, window, defer, variant, memo_bits, chunk;
 };
 
 Ctx& ctx();

@@ -37,7 +37,8 @@ struct BatchArgs {
     TurnK tk;          // constants of war_turn_fma
     int n, m, hbins, dbins, blk, W, half, sample, distinct, defer;
     u64* memo;         // cycle memo table (2^memo_bits words, 0 = empty), or null
-    u32 memo_bits, memo_pad;
+    u32 memo_bits;
+    u32 chunk;         // work units a lane takes from the counter at a time (0 or 1: one)
 };
 
 struct CycleWalk { u32 c1, c2; bool sym, on, is_min; };

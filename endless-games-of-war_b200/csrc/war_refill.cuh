@@ -31,6 +31,8 @@ struct Enum {
     u32 base;    // first permuted position, M - j
     u32 k, k0, k1;
     bool live;   // P (and k) name the next unplayed position
+    u64 cu;      // the next unit of the lane's chunk
+    u32 cleft;   // units of the chunk not taken yet
 };
 
 template <bool CANON>
@@ -46,8 +48,14 @@ __device__ __forceinline__ u32 heap_full(u32 j) {
 
 template <bool CANON>
 __device__ __forceinline__ bool fetch_unit(Enum& E, const BatchArgs& a, u64* counter) {
-    u64 u = atomicAdd(counter, 1ull);
-    if (u >= a.n_units) return false;
+    if (E.cleft == 0u) {   // the next chunk of consecutive units
+        const u32 c = a.chunk > 1u ? a.chunk : 1u;
+        E.cu = atomicAdd(counter, (u64)c);
+        E.cleft = c;
+    }
+    const u64 u = E.cu++;
+    E.cleft--;
+    if (u >= a.n_units) { E.cleft = 0u; return false; }   // the rest of the chunk lies beyond the list too
     u64 r;
     u32 j, k0, k1;
     if (u < a.main_count) {
@@ -152,6 +160,7 @@ __device__ __forceinline__ void refill_body(const BatchArgs& a, DevAcc* __restri
 
     Enum E;
     E.live = false;
+    E.cleft = 0u;
     Game<EXTRA, SHAPE> g[G];
     // Per-lane totals.  A launch plays fewer than 2^32 games in all, so no lane's 32-bit turn total wraps.
     u32 cyc = 0, done = 0, maxfin = 0, capped = 0, turns = 0;
@@ -494,6 +503,7 @@ __device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __res
 
     Enum E;
     E.live = false;
+    E.cleft = 0u;
     LGame<EXTRA, MEMO> g[G];
     u32 cyc = 0, done = 0, maxfin = 0, capped = 0, turns = 0;
     u32 sc = 0, scy = 0, slam = 0, slen = 0, smax = 0, oncyc = 0, dmin = 0;

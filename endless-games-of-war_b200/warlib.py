@@ -37,7 +37,7 @@ class Job(ctypes.Structure):
 class Tune(ctypes.Structure):
     _fields_ = [("threads", ctypes.c_int32), ("blocks_per_sm", ctypes.c_int32), ("games", ctypes.c_int32),
                 ("block_m", ctypes.c_int32), ("window", ctypes.c_int32), ("defer", ctypes.c_int32),
-                ("variant", ctypes.c_int32), ("memo_bits", ctypes.c_int32)]
+                ("variant", ctypes.c_int32), ("memo_bits", ctypes.c_int32), ("chunk", ctypes.c_int32)]
 
 
 class Result(ctypes.Structure):
@@ -161,8 +161,8 @@ def make_job(n, mode=DEALS, rule=0, flags=0, lo=0, hi=None, hbins=0, dbins=0, bl
     return Job(n, mode, rule, flags, hbins, dbins, blk, sample_ppm, lo, hi, seed)
 
 
-def make_tune(threads=0, blocks_per_sm=0, games=0, block_m=0, window=0, defer=0, variant=0, memo_bits=0):
-    return Tune(threads, blocks_per_sm, games, block_m, window, defer, variant, memo_bits)
+def make_tune(threads=0, blocks_per_sm=0, games=0, block_m=0, window=0, defer=0, variant=0, memo_bits=0, chunk=0):
+    return Tune(threads, blocks_per_sm, games, block_m, window, defer, variant, memo_bits, chunk)
 
 
 def enumerate_job(job, tune=None):

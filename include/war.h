@@ -79,7 +79,7 @@ typedef struct war_job {
 typedef struct war_tune {
     int32_t threads;       /* threads per block (multiple of 32, 64..1024) */
     int32_t blocks_per_sm; /* resident blocks per SM for the persistent grid */
-    int32_t games;         /* games in flight per thread: 1 or 2 */
+    int32_t games;         /* games in flight per thread: 1, 2, or 4 (4: variants 3 and 31 only, at most 256 threads) */
     int32_t block_m;       /* each work unit covers m! consecutive ranks (deals) or m! orders x splits (canon); 1..8 */
     int32_t window;        /* Brent first tortoise window (power of two); 1 = the reference's schedule */
     int32_t defer;         /* immediate records: lanes that wait, decided, before the warp refills them (1..32);
@@ -96,6 +96,8 @@ typedef struct war_tune {
                               with their outcome (n <= 16; canonical scans take only this form).
                               Every form gives the same results; out-of-range forms fall back to none. */
     int32_t memo_bits;     /* cycle memo: log2 of its 8-byte slots (12..31); 0 = 24 (128 MiB) */
+    int32_t chunk;         /* work units a lane takes from the work counter at a time (1..4096; 0 = 1): each lane
+                              walks chunks of chunk x block_m! consecutive ranks (deals) */
 } war_tune;
 
 /* Aggregates of one job.  Matches what gpu/war_gpu.py run() returns (gpu/war_gpu.py:346-352) before

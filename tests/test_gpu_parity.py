@@ -86,7 +86,10 @@ def test_random_ranges(wl, oracle, mode):
                                   dict(variant=7, games=2, defer=8), dict(variant=6, threads=128, defer=4),
                                   dict(variant=7, window=1, memo_bits=12, defer=32), dict(variant=15, games=1, defer=16),
                                   dict(variant=14, games=2, threads=512, memo_bits=14), dict(variant=31, games=1, defer=16),
-                                  dict(variant=30, games=2, memo_bits=13, defer=4)])
+                                  dict(variant=30, games=2, memo_bits=13, defer=4),
+                                  dict(variant=31, games=4, threads=256, defer=8), dict(variant=3, games=4, threads=128, defer=4),
+                                  dict(variant=31, chunk=64, defer=8), dict(variant=31, chunk=7, games=2, memo_bits=16),
+                                  dict(variant=3, chunk=1456, block_m=4), dict(chunk=3, block_m=8)])
 def test_tunes_agree(wl, oracle, tune):
     for job in (wl.make_job(11, rule=0, hbins=64), wl.make_job(10, wl.CANON, rule=1, flags=wl.F_DISTINCT | wl.F_SHAPE,
                                                                  hbins=256, dbins=64)):
@@ -171,6 +174,15 @@ def test_floyd_full_range_canon13(wl, golden):
     g = golden["canon_rule0"][13]
     assert (f.s_count, f.s_cyc, f.s_maxfin) == (g["positions"], g["cycling"], g["longest"])
     assert floyd_key(f) == floyd_key(wl.enumerate_job(job))
+
+
+def test_four_games_only_for_the_product_variants(wl):
+    """Four games per lane are compiled for variants 3 and 31 only; other variants refuse them."""
+    job = wl.make_job(10, hbins=32)
+    with pytest.raises(wl.WarError):
+        wl.enumerate_job(job, wl.make_tune(games=4, variant=7, threads=256, defer=8))
+    with pytest.raises(wl.WarError):
+        wl.enumerate_job(job, wl.make_tune(chunk=5000))
 
 
 def test_native_autotune_keeps_counts(wl, oracle):
