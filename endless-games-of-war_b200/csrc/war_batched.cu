@@ -15,6 +15,12 @@ __global__ void __launch_bounds__(G == 1 ? 1024 : (G == 2 ? 512 : 256)) batched_
 
 typedef void (*BatchedFn)(const BatchArgs, DevAcc*);
 
+// Dynamic shared memory of a block: the cycle-length and ending-length histograms (u32 bins), then one
+// 8-byte chunk cursor per thread (chunk_cursor in war_refill.cuh).
+static size_t batched_shmem(int hbins, int threads) {
+    return sizeof(u32) * (size_t)((hbins + WAR_EBINS + 1) & ~1) + sizeof(u64) * (size_t)threads;
+}
+
 template <int RULE, int G, int V>
 static BatchedFn pick_g(int canon, int shape, int extra) {
     if (!canon) return extra ? batched_kernel<RULE, G, false, false, true, V> : batched_kernel<RULE, G, false, false, false, V>;
@@ -58,8 +64,7 @@ cudaError_t launch_batched(const BatchArgs& a, int canon, int rule, int shape, c
     int extra = (a.distinct || a.sample) ? 1 : 0;
     BatchedFn fn = pick(canon, rule, canon && shape, extra, bs.games, bs.variant);
     if (!fn) return cudaErrorInvalidConfiguration;
-    size_t shmem = sizeof(u32) * (size_t)(a.hbins + WAR_EBINS);
-    fn<<<bs.blocks, bs.threads, shmem, st>>>(a, acc);
+    fn<<<bs.blocks, bs.threads, batched_shmem(a.hbins, bs.threads), st>>>(a, acc);
     note_launch();
     return cudaGetLastError();
 }
@@ -69,8 +74,8 @@ int batched_max_blocks_per_sm(int canon, int rule, int shape, int distinct, int 
     BatchedFn fn = pick(canon, rule, canon && shape, (distinct || sample) ? 1 : 0, games, variant);
     if (!fn) return 0;   // a combination that is not compiled (four games per lane outside variants 3 and 31)
     int nb = 0;
-    size_t shmem = sizeof(u32) * (size_t)(hbins + WAR_EBINS);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, threads, shmem) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, threads, batched_shmem(hbins, threads)) != cudaSuccess)
+        return 0;
     return nb;
 }
 

@@ -31,9 +31,17 @@ struct Enum {
     u32 base;    // first permuted position, M - j
     u32 k, k0, k1;
     bool live;   // P (and k) name the next unplayed position
-    u64 cu;      // the next unit of the lane's chunk
-    u32 cleft;   // units of the chunk not taken yet
 };
+
+// With a.chunk > 1 a lane takes that many consecutive units from the counter at a time.  Its cursor (the next
+// unit of its chunk) lives in shared memory, one word per thread after the two histograms, so that the usual
+// one-unit path keeps no register for it.  Chunks start at multiples of a.chunk, so the cursor needs a new
+// chunk exactly when it is a multiple of a.chunk.
+__device__ __forceinline__ u64* chunk_cursor(const BatchArgs& a) {
+    extern __shared__ u32 war_dyn_sh[];
+    const u32 off = ((u32)a.hbins + (u32)WAR_EBINS + 1u) & ~1u;   // 8-byte aligned
+    return (u64*)(war_dyn_sh + off) + threadIdx.x;
+}
 
 template <bool CANON>
 __device__ __forceinline__ u32 pos_shift(u32 p) {
@@ -48,14 +56,15 @@ __device__ __forceinline__ u32 heap_full(u32 j) {
 
 template <bool CANON>
 __device__ __forceinline__ bool fetch_unit(Enum& E, const BatchArgs& a, u64* counter) {
-    if (E.cleft == 0u) {   // the next chunk of consecutive units
-        const u32 c = a.chunk > 1u ? a.chunk : 1u;
-        E.cu = atomicAdd(counter, (u64)c);
-        E.cleft = c;
+    u64 u;
+    if (a.chunk <= 1u) {
+        u = atomicAdd(counter, 1ull);
+    } else {
+        u64* cur = chunk_cursor(a);
+        if (*cur % a.chunk == 0ull) *cur = atomicAdd(counter, (u64)a.chunk);   // the next chunk
+        u = (*cur)++;
     }
-    const u64 u = E.cu++;
-    E.cleft--;
-    if (u >= a.n_units) { E.cleft = 0u; return false; }   // the rest of the chunk lies beyond the list too
+    if (u >= a.n_units) return false;   // (the counter only grows: later units lie beyond the list too)
     u64 r;
     u32 j, k0, k1;
     if (u < a.main_count) {
@@ -160,7 +169,7 @@ __device__ __forceinline__ void refill_body(const BatchArgs& a, DevAcc* __restri
 
     Enum E;
     E.live = false;
-    E.cleft = 0u;
+    if (a.chunk > 1u) *chunk_cursor(a) = 0ull;
     Game<EXTRA, SHAPE> g[G];
     // Per-lane totals.  A launch plays fewer than 2^32 games in all, so no lane's 32-bit turn total wraps.
     u32 cyc = 0, done = 0, maxfin = 0, capped = 0, turns = 0;
@@ -503,7 +512,7 @@ __device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __res
 
     Enum E;
     E.live = false;
-    E.cleft = 0u;
+    if (a.chunk > 1u) *chunk_cursor(a) = 0ull;
     LGame<EXTRA, MEMO> g[G];
     u32 cyc = 0, done = 0, maxfin = 0, capped = 0, turns = 0;
     u32 sc = 0, scy = 0, slam = 0, slen = 0, smax = 0, oncyc = 0, dmin = 0;
