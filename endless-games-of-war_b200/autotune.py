@@ -14,7 +14,7 @@ at a time, over
                    between services                                      (1..32)
     variant        bit 0: multiply-add turn form; bit 1: latched records serviced every `defer` iterations;
                    bit 2: cycle memo (deals); bit 3: the memo holds every cycle state; bit 4: and paths
-    memo_bits      log2 of the memo table's 8-byte words                 (26..30)
+    memo_bits      log2 of the memo table's 8-byte words                 (26..31)
 Every configuration must return exactly the same counts as the first one; a mismatch raises.  The best
 configuration is stored in tune_cache.json next to this file, keyed by GPU name, n, mode, rule and flags.
 
@@ -44,7 +44,7 @@ SPACE = {
     "window": [8, 16, 32, 64, 128],
     "defer": [1, 2, 4, 6, 8, 12, 16, 24, 32],
     "variant": [0, 1, 2, 3, 6, 7, 14, 15, 30, 31],
-    "memo_bits": [26, 28, 29, 30],
+    "memo_bits": [26, 28, 29, 30, 31],
 }
 DEFAULT = {"block_m": 5, "games": 2, "threads": 512, "blocks_per_sm": 0, "window": 32, "defer": 8, "variant": 1,
            "memo_bits": 24, "chunk": 1}

@@ -25,7 +25,7 @@ const std::vector<Dim>& dims() {
         {"window", &war_tune::window, {8, 16, 32, 64, 128}},
         {"defer", &war_tune::defer, {1, 2, 4, 8, 12, 16, 24, 32}},
         {"variant", &war_tune::variant, {0, 1, 2, 3, 6, 7, 14, 15, 30, 31}},
-        {"memo_bits", &war_tune::memo_bits, {24, 26, 28, 30}},
+        {"memo_bits", &war_tune::memo_bits, {24, 26, 28, 30, 31}},
         {"chunk", &war_tune::chunk, {1, 8, 64, 512, 1456}},
     };
     return d;
