@@ -38,9 +38,10 @@ sys.path.insert(0, PKG)
 # under the winner: 22), Brent's test and bookkeeping (6), the end test (2).  Fixed from the source of
 # war_turn / batched_kernel, not from compiled code.
 K_OPS_PER_TURN = 30
-# DRAM bytes (read + write) per deal of the path-memo refill kernel, from an ncu capture of the second span
-# of `war_gpu.py 13 --hist 256` (1.94e9 deals, 214.6 GB): the random memo reads cost ~108 B each.
-MEMO_DRAM_BYTES_PER_DEAL = 110.8
+# DRAM bytes (read + write) per deal of the path-memo refill kernel at this line's configuration (all 13!
+# deals, 8 GiB table): one-pass ncu capture of both launches of a timed step, 697.3 GB read and 13.1 GB
+# written for 6,227,020,800 deals (112.0 + 2.1 B per deal); each random 8-byte lookup costs a DRAM line.
+MEMO_DRAM_BYTES_PER_DEAL = 114.1
 # Turns of the reference's own schedule (Brent with the tortoise saved at powers of two from the first turn)
 # over all 13! deals, as counted by an instrumented copy of cpu/war.cpp; the plain kernel reproduces it
 # exactly (its `turns`).
