@@ -65,3 +65,22 @@ def test_space_sizes():
     assert warlib.space_size(13) == math.factorial(13)
     assert warlib.space_size(14, warlib.CANON) == math.factorial(13) * 13
     assert warlib.space_size(1, warlib.CANON) == 0
+
+
+def test_bench_counts_the_extra_units_the_library_plans():
+    """bench.py's e2e line counts the bytes of the extra work units copied to the device per step; its count
+    of units for a deal range equals the plan the library makes (war_plan, host only)."""
+    import random
+    import sys
+    import os
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+    import warlib
+    rnd = random.Random(3)
+    for _ in range(300):
+        n = rnd.randint(6, 16)
+        m = rnd.randint(1, min(8, n))
+        total = warlib.space_size(n)
+        lo = rnd.randrange(total)
+        hi = min(total, lo + rnd.choice([1, 50, 5000, 10 ** 6, 10 ** 9, total]))
+        assert bench.deal_extra_units(lo, hi, m) == len(warlib.plan(warlib.make_job(n, lo=lo, hi=hi), m)[2])
