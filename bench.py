@@ -562,6 +562,15 @@ def main():
                         "peak_source": "war_measure_gather_peak on this GPU (random ld.global.cg of 8 bytes from a "
                                        "table of the memo's size, measured)",
                         "int_issue": int_issue}
+            if mode == 0 and n == 13:
+                # the same kernel against the copy bandwidth: its algorithmic bytes (8 per lookup or store) and
+                # the DRAM bytes it actually moves (ncu, per deal), per second of kernel time
+                hbm_peak, hbm_src = measured_hbm_peak()
+                dram_gbs = MEMO_DRAM_BYTES_PER_DEAL * total / (kernel_ms * 1e-3) / 1e9
+                roofline["hbm"] = {"achieved_algorithmic_GBps": memo["algorithmic_GBps"],
+                                   "achieved_dram_GBps": dram_gbs, "peak_GBps": hbm_peak,
+                                   "frac_algorithmic": memo["algorithmic_GBps"] / hbm_peak,
+                                   "frac_dram": dram_gbs / hbm_peak, "peak_source": hbm_src}
         else:
             roofline = dict(int_issue, bound="int_issue", traffic=None,
                             traffic_unit="DRAM bytes per launch: accumulators only (no table)")
