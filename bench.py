@@ -231,13 +231,22 @@ def _oracle_sample_rate(w, target_s, cores, seed=0):
     n, mode = w["n"], w["mode"]
     total = space(n, mode)
 
+    engine = w.get("engine", "refill")
+    # the space the workload samples: its own slice for the 17-card workloads, else the whole rank space
+    base, total = (w["lo"], w["hi"] - w["lo"]) if engine != "refill" else (0, total)
+
     def run(slice_len):
         t0 = time.time()
         for i in range(64):
-            lo = (total // 64) * i + (seed * 7919) % max(1, total // 64 - slice_len)
-            job = oracle.make_job(n, mode, 0, w["flags"] & ~8, lo, min(total, lo + slice_len), hbins=w["hbins"],
+            lo = base + (total // 64) * i + (seed * 7919) % max(1, total // 64 - slice_len)
+            job = oracle.make_job(n, mode, 0, w["flags"] & ~8, lo, min(base + total, lo + slice_len), hbins=w["hbins"],
                                   dbins=w.get("dbins", 0))
-            oracle.enumerate_job(job, cores)
+            if engine == "held":      # the restatement of gpu/war17.py
+                oracle.enumerate_held(job, cores)
+            elif engine == "wide":    # the restatement of gpu/war24.py with the workload's cycle test
+                oracle.war24(job, det=w["det"], window=32 if w["det"] == 0 else 1, threads=cores)
+            else:                     # the restatement of cpu/war.cpp / gpu/war_gpu.py
+                oracle.enumerate_job(job, cores)
         return time.time() - t0
 
     probe = 4096
@@ -252,10 +261,12 @@ def cpu_baseline(w, target_s=12.0):
     cores = os.cpu_count() or 1
     v, slice_len = _oracle_sample_rate(w, target_s, cores)
     mode = w["mode"]
+    what = {"held": "gpu/war17.py's", "wide": "gpu/war24.py's"}.get(w.get("engine"), "cpu/war.cpp's")
     return {"value": v, "unit": "positions/s" if mode else "deals/s", "cores": cores, "kind": "port",
-            "sample": "64 strided slices of %d ranks of the %s space, oracle/war_oracle.c (restatement of "
-                      "cpu/war.cpp's algorithm, OpenMP on all host threads), ~%.0f s" % (
-                          slice_len, "canonical-position" if mode else "deal", target_s)}
+            "sample": "64 strided slices of %d ranks of the %s, oracle/war_oracle.c (restatement of "
+                      "%s algorithm, OpenMP on all host threads), ~%.0f s" % (
+                          slice_len, "workload's slice" if "engine" in w else
+                          ("canonical-position space" if mode else "deal space"), what, target_s)}
 
 
 def deal_extra_units(lo, hi, m):
@@ -399,11 +410,11 @@ def main():
     torch.cuda.set_device(local)
     stream = torch.cuda.current_stream()
     warlib.set_stream(stream.cuda_stream)
-    tune = war_gpu._tune_for(n, mode == 1, 0, w["flags"])
+    engine = w.get("engine", "refill")
+    # the 17-card engines run with their own defaults (war_enumerate_held / war_enumerate_wide, tune NULL)
+    tune = war_gpu._tune_for(n, mode == 1, 0, w["flags"]) if engine == "refill" else None
 
     floyd_ms = []
-
-    engine = w.get("engine", "refill")
 
     def step():
         if engine == "wide":

@@ -510,19 +510,26 @@ int war_enumerate_held(const war_job* job, const war_tune* tune, war_result* out
     if (job->lo == job->hi) return WAR_OK;
     int st;
     if ((st = ensure_ready())) return st;
-    const int threads = (tune && tune->threads) ? tune->threads : 256;
+    const bool memo = tune && (tune->variant & 4);   // the path memo (any variant with bit 2)
+    const int threads = (tune && tune->threads) ? tune->threads : (memo ? 256 : 512);
     const int block_m = std::min(job->n, (tune && tune->block_m) ? tune->block_m : 6);
     const int W = (tune && tune->window) ? tune->window : 32;
-    const int defer = (tune && tune->defer) ? tune->defer : 16;
-    const bool memo = tune && (tune->variant & 4);   // the path memo (any variant with bit 2)
+    const int defer = (tune && tune->defer) ? tune->defer : (memo ? 16 : 32);
     const int memo_bits = (tune && tune->memo_bits) ? tune->memo_bits : 28;
     if (memo && (memo_bits < 12 || memo_bits > 31)) return fail(WAR_EINVAL, "tune.memo_bits=%d (12..31)", memo_bits);
     if (threads < 64 || threads > 1024 || (threads & 31)) return fail(WAR_EINVAL, "tune.threads=%d", threads);
     if (block_m < 1 || block_m > 8) return fail(WAR_EINVAL, "tune.block_m=%d (1..8)", block_m);
     if (W < 1 || W > (1 << 16) || (W & (W - 1))) return fail(WAR_EINVAL, "tune.window=%d", W);
     if (defer < 1 || defer > 32) return fail(WAR_EINVAL, "tune.defer=%d (1..32)", defer);
-    const bool fma = tune && (tune->variant & 1);   // the multiply-add, branch-free turn
-    const int maxb = held_max_blocks_per_sm(job->rule, threads, job->hbins, memo, fma);
+    // the turn (variant & 3): 0 the counts packed in one word with multiply-add card arithmetic (the default),
+    // 1 multiply-adds on separate counts, 2 packed counts in logic/shift form, 3 the plain branching turn of
+    // gpu/war17.py; bit 3 tests the tortoise checkpoint after every turn instead of saving it at the services
+    static const int form_of_variant[4] = {3, 1, 2, 0};
+    const int form = form_of_variant[tune ? (tune->variant & 3) : 0];
+    HeldArgs a;
+    memset(&a, 0, sizeof a);
+    a.W = W; a.defer = defer; a.form = form; a.svc_off = (tune && (tune->variant & 8)) ? 1 : 0;
+    const int maxb = held_max_blocks_per_sm(job->rule, threads, job->hbins, memo, form, held_svc(a));
     if (maxb < 1) return fail(WAR_EINVAL, "launch shape threads=%d does not fit an SM%s", threads,
                               memo ? " (at most 512 with the memo)" : "");
     const int bps = (tune && tune->blocks_per_sm) ? std::min(tune->blocks_per_sm, maxb) : maxb;
@@ -536,12 +543,9 @@ int war_enumerate_held(const war_job* job, const war_tune* tune, war_result* out
         (e = cudaMemcpyAsync(c.d_units, p.extra.data(), sizeof(Unit) * p.extra.size(), cudaMemcpyHostToDevice,
                              cur_stream())) != cudaSuccess)
         return cuda_fail(e, "copy units");
-    HeldArgs a;
-    memset(&a, 0, sizeof a);
     for (int i = 0; i <= 17; i++) a.fact[i] = fact(i);
-    a.n = job->n; a.m = block_m; a.rule = job->rule; a.hbins = job->hbins; a.W = W; a.defer = defer;
+    a.n = job->n; a.m = block_m; a.rule = job->rule; a.hbins = job->hbins;
     a.units = c.d_units;
-    a.fma = fma ? 1 : 0;
     a.tk.k16 = 16u; a.tk.km16 = (u32)-16; a.tk.k2p28 = 1u << 28; a.tk.k4 = 4u; a.tk.one = 1u;
     if (memo) {
         if ((st = prepare_memo(c, job, memo_bits, 1, &a.memo))) return st;

@@ -175,6 +175,61 @@ __device__ __forceinline__ bool h_turn_fma(u64& wh, u64& wo, u32& lh, u32& lo, u
     return lo == 0u;
 }
 
+// The same turn on a packed count word s = 4 lh + 256 p (lh < 64 cards, so the fields never overlap); the
+// opponent's count is n - 1 - lh and is not kept.  Branch-free: when card n-1 is on top (s < 256) the
+// holder's pop is undone by a select and only the opponent's card goes under its pile.  Brent's test then
+// compares three words (wh, wo, s) instead of five, and the game is over exactly when the holder wins the
+// opponent's last card (lh = n - 2 before the turn), so no count has to be tested after it.  n4m8 = 4n - 8.
+template <int RULE>
+__device__ __forceinline__ bool h_turn_packed(u64& wh, u64& wo, u32& s, u32 n4m8) {
+    const u32 q = s & 255u;                  // 4 lh
+    const bool z = s < 256u;                 // the holder plays card n-1
+    const u32 c = (u32)wo & 15u, h = (u32)wh & 15u;
+    const u64 ws = wh >> 4;
+    wo >>= 4;
+    const bool hw = z | (h > c);             // the holder wins the turn
+    const u32 hi = max(h, c), lw = min(h, c);
+    const u32 pair = RULE ? (lw | (hi << 4)) : (hi | (lw << 4));
+    const u32 t = z ? c : pair;              // what goes under the winner's pile
+    const u32 pos = hw ? (z ? q : q - 4u) : n4m8 - q;
+    const u64 x = shl64((u64)t, pos);
+    const u64 m = hw ? ~0ull : 0ull;
+    wh = (z ? wh : ws) | (x & m);
+    wo = wo | (x & ~m);
+    // z: lh + 1 cards, card n-1 at depth lh (rule 0: above the captured card) or lh + 1 (rule 1);
+    // else: one card popped from each pile, two added to the winner's, card n-1 one place higher
+    s = z ? q * 65u + (4u + 256u * (u32)RULE) : s - 260u + (hw ? 8u : 0u);
+    return hw & (q == n4m8);
+}
+
+// The packed-count turn with the card arithmetic of h_turn_fma: both tops popped by funnel shift and
+// multiply-high, the cards as lo - 16 lo', the pair by multiply-add, and what goes under the winner's pile
+// added by mad.wide with a 0/1 weight instead of masks, so about a third of the turn runs on the FMA pipe.
+template <int RULE>
+__device__ __forceinline__ bool h_turn_packed_fma(u64& wh, u64& wo, u32& s, u32 n4m8, const TurnK& K) {
+    const u32 ol = (u32)wo, oh = (u32)(wo >> 32), hl = (u32)wh, hh = (u32)(wh >> 32);
+    const u32 nol = __funnelshift_r(ol, oh, 4), noh = __umulhi(oh, K.k2p28);
+    const u32 nhl = __funnelshift_r(hl, hh, 4), nhh = __umulhi(hh, K.k2p28);
+    const u32 c = ol + nol * K.km16, h = hl + nhl * K.km16;   // the two top cards
+    const u32 q = s & 255u;
+    const bool z = s < 256u;
+    const bool hw = z | (h > c);
+    const u32 pa = RULE ? c + h * K.k16 : h + c * K.k16;      // the holder won with h
+    const u32 pb = RULE ? h + c * K.k16 : c + h * K.k16;      // the opponent won
+    const u32 t = z ? c : (hw ? pa : pb);
+    const u32 pos = hw ? (z ? q : q - 4u) : n4m8 - q;
+    const u64 x = shl64((u64)t, pos);
+    const u32 xl = (u32)x, xh = (u32)(x >> 32);
+    const u32 bh = hw ? 1u : 0u, bo = K.one - bh;
+    u64 ah = z ? wh : (((u64)nhh << 32) | nhl), ao = ((u64)noh << 32) | nol;
+    ah = (u64)xl * bh + ah;
+    ao = (u64)xl * bo + ao;
+    wh = ((u64)((u32)(ah >> 32) + xh * bh) << 32) | (u32)ah;
+    wo = ((u64)((u32)(ao >> 32) + xh * bo) << 32) | (u32)ao;
+    s = z ? q * 65u + (4u + 256u * (u32)RULE) : bh * 8u + (s - 260u);
+    return hw & (q == n4m8);
+}
+
 // Path-memo key of a held-out state (the entry format of war_refill.cuh: the key itself is not stored, the
 // slot and entry give it back).  The n-1 other cards in the order holder's then opponent's, the holder's
 // count lh and the depth p; the last card is the one missing.  At 17 cards that is 15 nibbles + 8 bits =
@@ -202,7 +257,12 @@ __device__ __noinline__ void h_store_cycle(u64* T, u32 bits, u64 wh, u64 wo, u32
     }
 }
 
-template <int RULE, bool MEMO, bool FMA>
+// FORM 0: h_turn (branches on card n-1 on top), 1: h_turn_fma, 2: h_turn_packed (the counts in one word),
+// 3: h_turn_packed_fma.
+// SVC: the window W is a multiple of the service period, so a game (which starts at a service and plays
+// `period` turns between services while undecided) reaches each tortoise checkpoint W, 3W, 7W, ... exactly at
+// a service; the checkpoint is then saved there instead of being tested after every turn.
+template <int RULE, bool MEMO, int FORM, bool SVC>
 __global__ void __launch_bounds__(MEMO ? 512 : 1024) held_kernel(const __grid_constant__ HeldArgs a,
                                                                 DevAcc* __restrict__ acc) {
     extern __shared__ u32 sh[];
@@ -211,7 +271,7 @@ __global__ void __launch_bounds__(MEMO ? 512 : 1024) held_kernel(const __grid_co
     for (int b = threadIdx.x; b < a.hbins + WAR_EBINS; b += blockDim.x) sh[b] = 0;
     __syncthreads();
 
-    const u32 n = (u32)a.n, W = (u32)a.W;
+    const u32 n = (u32)a.n, W = (u32)a.W, n4m8 = 4u * n - 8u;
     const TurnK K = a.tk;
     const u32 hb1 = a.hbins > 0 ? (u32)(a.hbins - 1) : 0u;
     const int period = a.defer > 4 ? (a.defer + 3) & ~3 : 4;
@@ -221,6 +281,7 @@ __global__ void __launch_bounds__(MEMO ? 512 : 1024) held_kernel(const __grid_co
     E.live = false;
     u64 wh = 0, wo = 0, th = 0, to = 0;
     u32 lh = 0, lo = 0, p = 0, tlh = 0, tp = 0, rounds = 0, next = 0;
+    u32 s = 0, ts = 0;   // FORM 2, 3: 4 lh + 256 p
     bool done = true, kcy = false, active = false;
     u32 cyc = 0, ndone = 0, maxfin = 0, capped = 0, turns = 0;
     // the path memo (war_refill.cuh): lookups at every service, the game's last two misses stored with
@@ -231,6 +292,14 @@ __global__ void __launch_bounds__(MEMO ? 512 : 1024) held_kernel(const __grid_co
     u64 ka = 0, kb = 0;
     u32 ta = 0, tb = 0, mv = 0, mlook = 0, mhit = 0, mstore = 0;
 
+    auto unpack = [&]() {   // FORM 2, 3: the counts of the current state
+        if (FORM >= 2) { lh = (s & 255u) >> 2; p = s >> 8; lo = n - 1u - lh; }
+    };
+    auto save = [&]() {     // the tortoise checkpoint
+        th = wh; to = wo;
+        if (FORM >= 2) ts = s; else { tlh = lh; tp = p; }
+        next = 2u * next + W;
+    };
     auto start_game = [&]() {
         active = false;
         for (;;) {
@@ -241,7 +310,8 @@ __global__ void __launch_bounds__(MEMO ? 512 : 1024) held_kernel(const __grid_co
         }
         active = true;
         ndone++;
-        th = wh; to = wo; tlh = lh; tp = p;
+        s = 4u * lh + 256u * p;
+        th = wh; to = wo; tlh = lh; tp = p; ts = s;
         rounds = 0; next = W; kcy = false;
         ta = 0u; tb = 0u; mv = 0u;
         done = lo == 0u;   // n = 1 only (never here: n >= 2)
@@ -251,20 +321,33 @@ __global__ void __launch_bounds__(MEMO ? 512 : 1024) held_kernel(const __grid_co
     bool running = __any_sync(WAR_FULL_MASK, active);
     while (running) {
         for (int k = 0; k < period; k++) {
-            bool en = FMA ? h_turn_fma<RULE>(wh, wo, lh, lo, p, K) : h_turn<RULE>(wh, wo, lh, lo, p);
-            if (!done) rounds++;
-            const bool cy = (wh == th) & (wo == to) & (lh == tlh) & (p == tp);
-            en = en | (lo == 0u);
-            const bool fin = (cy | en) & !done;
-            kcy = fin ? (cy & !en) : kcy;
-            done = done | fin;
-            if (lo == 0u) { lo = 1u; wo = 0ull; }   // a finished game keeps being stepped harmlessly
-            if (rounds == next && !done) {
+            if (FORM >= 2) {
+                const bool en = FORM == 3 ? h_turn_packed_fma<RULE>(wh, wo, s, n4m8, K) : h_turn_packed<RULE>(wh, wo, s, n4m8);
+                if (!done) rounds++;
+                const bool cy = (wh == th) & (wo == to) & (s == ts);
+                kcy = done ? kcy : (cy & !en);
+                done = done | cy | en;
+            } else {
+                bool en = FORM == 1 ? h_turn_fma<RULE>(wh, wo, lh, lo, p, K) : h_turn<RULE>(wh, wo, lh, lo, p);
+                if (!done) rounds++;
+                const bool cy = (wh == th) & (wo == to) & (lh == tlh) & (p == tp);
+                en = en | (lo == 0u);
+                const bool fin = (cy | en) & !done;
+                kcy = fin ? (cy & !en) : kcy;
+                done = done | fin;
+                if (lo == 0u) { lo = 1u; wo = 0ull; }   // a finished game keeps being stepped harmlessly
+            }
+            if (!SVC && rounds == next && !done) {
                 if (next > WAR_TURN_CAP) { capped++; done = true; active = false; }
-                else { th = wh; to = wo; tlh = lh; tp = p; next = 2u * next + W; }
+                else save();
             }
         }
+        if (SVC && rounds == next && !done) {
+            if (next > WAR_TURN_CAP) { capped++; done = true; active = false; }
+            else save();
+        }
         if (memo != nullptr) {
+            unpack();
             const bool look = active & !done;
             const u64 key = h_key(wh, wo, lh, p, n);
             const u64 e = look ? __ldcg((const unsigned long long*)memo + memo_slot(key, mbits)) : 0ull;
@@ -295,7 +378,8 @@ __global__ void __launch_bounds__(MEMO ? 512 : 1024) held_kernel(const __grid_co
                         const u64 v = kcy ? 2ull * lam : 2ull * (len - tb) + 1ull;
                         if (v <= vmask) { __stcg((unsigned long long*)memo + memo_slot(kb, mbits), path_entry(kb, mbits, v)); mstore++; }
                     }
-                    if (kcy && mcy == 0u) {   // found by Brent: store its cycle
+                    if (kcy && mcy == 0u) {   // found by Brent: store its cycle (the game is still on it)
+                        unpack();
                         h_store_cycle<RULE>(memo, mbits, wh, wo, lh, lo, p, n, lam);
                         mstore += lam;
                     }
@@ -333,25 +417,37 @@ __global__ void __launch_bounds__(MEMO ? 512 : 1024) held_kernel(const __grid_co
 
 typedef void (*HeldFn)(const HeldArgs, DevAcc*);
 
-static HeldFn held_pick(int rule, bool memo, bool fma) {
-    if (rule) return memo ? (fma ? held_kernel<1, true, true> : held_kernel<1, true, false>)
-                          : (fma ? held_kernel<1, false, true> : held_kernel<1, false, false>);
-    return memo ? (fma ? held_kernel<0, true, true> : held_kernel<0, true, false>)
-                : (fma ? held_kernel<0, false, true> : held_kernel<0, false, false>);
+template <int RULE, bool MEMO>
+static HeldFn held_pick_form(int form, bool svc) {
+    if (form == 3) return svc ? held_kernel<RULE, MEMO, 3, true> : held_kernel<RULE, MEMO, 3, false>;
+    if (form == 2) return svc ? held_kernel<RULE, MEMO, 2, true> : held_kernel<RULE, MEMO, 2, false>;
+    if (form == 1) return svc ? held_kernel<RULE, MEMO, 1, true> : held_kernel<RULE, MEMO, 1, false>;
+    return svc ? held_kernel<RULE, MEMO, 0, true> : held_kernel<RULE, MEMO, 0, false>;
+}
+
+// The checkpoint can be saved at the services when W is a multiple of the service period.
+bool held_svc(const HeldArgs& a) {
+    const int period = a.defer > 4 ? (a.defer + 3) & ~3 : 4;
+    return !a.svc_off && a.W % period == 0;
+}
+
+static HeldFn held_pick(int rule, bool memo, int form, bool svc) {
+    if (rule) return memo ? held_pick_form<1, true>(form, svc) : held_pick_form<1, false>(form, svc);
+    return memo ? held_pick_form<0, true>(form, svc) : held_pick_form<0, false>(form, svc);
 }
 
 cudaError_t launch_held(const HeldArgs& a, int threads, int blocks, DevAcc* acc, cudaStream_t st) {
     const size_t shmem = sizeof(u32) * (size_t)(a.hbins + WAR_EBINS);
-    held_pick(a.rule, a.memo != nullptr, a.fma != 0)<<<blocks, threads, shmem, st>>>(a, acc);
+    held_pick(a.rule, a.memo != nullptr, a.form, held_svc(a))<<<blocks, threads, shmem, st>>>(a, acc);
     note_launch();
     return cudaGetLastError();
 }
 
-int held_max_blocks_per_sm(int rule, int threads, int hbins, bool memo, bool fma) {
+int held_max_blocks_per_sm(int rule, int threads, int hbins, bool memo, int form, bool svc) {
     if (memo && threads > 512) return 0;
     int nb = 0;
     const size_t shmem = sizeof(u32) * (size_t)(hbins + WAR_EBINS);
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, held_pick(rule, memo, fma), threads, shmem);
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, held_pick(rule, memo, form, svc), threads, shmem);
     return e == cudaSuccess ? nb : 0;
 }
 

@@ -138,11 +138,14 @@ struct HeldArgs {
     int n, m, rule, hbins, W, defer;
     u64* memo;        // path memo (2^memo_bits words, 0 = empty), or null
     u32 memo_bits;
-    int fma;          // the multiply-add, branch-free turn (h_turn_fma)
+    int form;         // the turn: 0 h_turn, 1 h_turn_fma (multiply-add), 2 h_turn_packed (counts in one word),
+                      // 3 h_turn_packed_fma
+    int svc_off;      // test the tortoise checkpoint after every turn even where it could be saved at the services
     TurnK tk;         // its constants
 };
 cudaError_t launch_held(const HeldArgs& a, int threads, int blocks, DevAcc* acc, cudaStream_t st);
-int held_max_blocks_per_sm(int rule, int threads, int hbins, bool memo, bool fma);
+int held_max_blocks_per_sm(int rule, int threads, int hbins, bool memo, int form, bool svc);
+bool held_svc(const HeldArgs& a);
 
 struct FloydArgs {
     u64 fact[17];

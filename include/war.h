@@ -207,9 +207,14 @@ typedef struct war_job_status {
  * so it is kept out of the packed piles and tracked by its depth in its holder's pile; that keeps 17
  * cards in 4-bit nibbles.  Same job and result as war_enumerate for deals (cycling count, longest ending
  * game, cycle-length and ending-length histograms, turns), both rules; only WAR_F_MEMO_KEEP applies.
- * tune: threads, blocks_per_sm, block_m, window, defer; variant bit 0 = a branch-free multiply-add turn
- * (same results, measured the same speed), bit 2 = the path memo with memo_bits (0 = 28), at most 512
- * threads then; NULL = defaults (no memo).  war_enumerate sends n = 17 deal jobs here. */
+ * tune: threads (0 = 512, 256 with the memo), blocks_per_sm, block_m (0 = 6), window (0 = 32), defer
+ * (turns between services, 0 = 32, 16 with the memo); variant bits 0-1 pick the turn, all with the same
+ * results: 0 = the two counts packed in one word with multiply-add card arithmetic (the default and the
+ * fastest), 1 = multiply-adds on separate counts, 2 = packed counts in logic/shift form, 3 = the plain
+ * branching turn of gpu/war17.py; bit 2 = the path memo with memo_bits (0 = 28), at most 512 threads then;
+ * bit 3 = test Brent's checkpoint after every turn (by default it is saved at the services whenever the
+ * window is a multiple of the service period).  NULL = defaults (no memo).  war_enumerate sends n = 17 deal
+ * jobs here. */
 int war_enumerate_held(const war_job* job, const war_tune* tune, war_result* out);
 
 /* The 5-bit-pile engine (gpu/war24.py): deals of 2..20 cards (deal ranks are 64-bit), cards of 5 bits in

@@ -20,9 +20,14 @@ def oracle_held(oracle, n, rule=0, lo=0, hi=None, hbins=128):
     return oracle.to_dict(oracle.enumerate_held(oracle.make_job(n, 0, rule, 0, lo, hi, hbins)))
 
 
-@pytest.mark.parametrize("rule,variant", [(0, 0), (1, 0), (0, 1), (1, 1)])
+# tune.variant of the held-out engine, bits 0-1 the turn: 0 counts packed in one word with multiply-add card
+# arithmetic (the default), 1 multiply-adds on separate counts, 2 packed counts in logic/shift form, 3 the plain
+# branching turn of gpu/war17.py; bit 2 the path memo; bit 3 the tortoise checkpoint tested after every turn
+# (else saved at the services where the window is a multiple of the service period)
+@pytest.mark.parametrize("rule,variant", [(r, v) for r in (0, 1) for v in (0, 1, 2, 3, 8, 9, 10, 11)])
 def test_small_n_full_against_oracle_and_main_engine(wl, oracle, rule, variant):
-    """Every deal of n <= 11, both turn forms of the held-out engine (variant 1: multiply-add, branch-free)."""
+    """Every deal of n <= 11, every turn form of the held-out engine, with the checkpoint saved at the services
+    and (variants 8..11) after every turn."""
     for n in range(2, 12):
         got = held(wl, n, rule, tune=wl.make_tune(variant=variant))
         want = oracle_held(oracle, n, rule)
@@ -72,7 +77,10 @@ def test_n17_through_war_enumerate_and_tunes(wl, oracle):
         assert got[k] == want[k], k
     for t in (dict(threads=128), dict(threads=1024, defer=4), dict(block_m=3, defer=16), dict(block_m=8, window=1),
               dict(blocks_per_sm=1, window=128), dict(variant=1), dict(variant=1, threads=1024, rule=0),
-              dict(variant=5, memo_bits=20)):
+              dict(variant=5, memo_bits=20), dict(variant=2), dict(variant=2, defer=12), dict(variant=10),
+              dict(variant=2, window=1, block_m=5), dict(variant=6, memo_bits=20), dict(variant=4, memo_bits=20),
+              dict(variant=3), dict(variant=3, defer=32), dict(variant=3, defer=20), dict(variant=11),
+              dict(variant=3, window=8, defer=12), dict(variant=7, memo_bits=20), dict(variant=15, memo_bits=20)):
         t.pop("rule", None)
         got = held(wl, 17, 0, lo, hi, 256, wl.make_tune(**t))
         for k in FIELDS:
@@ -88,17 +96,17 @@ def test_refusals(wl):
 
 
 def memo_held(wl, bits=24, **kw):
-    t = dict(variant=31, threads=256, memo_bits=bits)
+    t = dict(variant=4, threads=256, memo_bits=bits)   # the default turn with the path memo
     t.update(kw)
     return wl.make_tune(**t)
 
 
-@pytest.mark.parametrize("bits", [12, 24])
-def test_memo_small_n_and_slices(wl, oracle, bits):
+@pytest.mark.parametrize("bits,variant", [(12, 4), (24, 4), (24, 5), (24, 6), (24, 7), (12, 7)])
+def test_memo_small_n_and_slices(wl, oracle, bits, variant):
     """The held-out engine with the path memo (its own 63/64-bit state keys) against the oracle: every deal
     of n <= 11, slices of n = 14..17, and a table far too small (2^12 words)."""
     for n in range(4, 12):
-        got, want = held(wl, n, n & 1, tune=memo_held(wl, bits)), oracle_held(oracle, n, n & 1)
+        got, want = held(wl, n, n & 1, tune=memo_held(wl, bits, variant=variant)), oracle_held(oracle, n, n & 1)
         for k in FIELDS:
             assert got[k] == want[k], (n, k)
     rnd = random.Random(bits)
@@ -107,7 +115,7 @@ def test_memo_small_n_and_slices(wl, oracle, bits):
         lo = rnd.randrange(0, math.factorial(n) - 10 ** 6)
         hi = lo + rnd.choice([777, 300001, 10 ** 6])
         rule = rnd.randint(0, 1)
-        got, want = held(wl, n, rule, lo, hi, 256, memo_held(wl, bits)), oracle_held(oracle, n, rule, lo, hi, 256)
+        got, want = held(wl, n, rule, lo, hi, 256, memo_held(wl, bits, variant=variant)), oracle_held(oracle, n, rule, lo, hi, 256)
         for k in FIELDS:
             assert got[k] == want[k], (n, lo, hi, k)
 
