@@ -573,13 +573,23 @@ __device__ __forceinline__ void refill_latched(const BatchArgs& a, DevAcc* __res
                     const bool fin = (cy | en) & !x.done;
                     x.kcy = fin ? cy : x.kcy;
                     x.done = x.done | fin;
-                    if (x.rounds == x.next && !x.done) {
-                        if (x.next > WAR_TURN_CAP) {   // abandon (never expected): counted, slot serviced as done
-                            capped++; x.done = true; x.st = ST_WAITING;
-                        } else {
-                            x.t1 = x.w1; x.t2 = x.w2; x.next = 2u * x.next + W;
-                        }
-                    }
+                }
+            }
+        }
+        // Brent's checkpoint, at the service: a game starts at a service and plays `period` turns between
+        // services while undecided, so when W is a multiple of the period the checkpoints W, 3W, 7W, ... all
+        // fall on services and this is the reference's doubling schedule (with first window W) exactly; else
+        // the tortoise is saved at the first service at or after the checkpoint.  next = 2 t + W keeps the turn
+        // t of the last save ((next - W) / 2 names it; the gaps still double, so every cycle is found, and
+        // the first return to the saved state is exactly one cycle length after it).
+#pragma unroll
+        for (int i = 0; i < G; i++) {
+            LGame<EXTRA, MEMO>& x = g[i];
+            if (!x.done && x.rounds >= x.next) {
+                if (x.next > WAR_TURN_CAP) {   // abandon (never expected): counted, slot serviced as done
+                    capped++; x.done = true; x.st = ST_WAITING;
+                } else {
+                    x.t1 = x.w1; x.t2 = x.w2; x.next = 2u * x.rounds + W;
                 }
             }
         }
