@@ -379,6 +379,9 @@ def main():
     ap.add_argument("--no-serving", action="store_true", help="skip the serving leg")
     ap.add_argument("--serving-jobs", type=int, default=600)
     ap.add_argument("--serving-rate", type=float, default=20.0)
+    ap.add_argument("--tune", default=None,
+                    help='JSON object overriding fields of the stored tune of the refill engine, e.g. '
+                         '\'{"variant": 3}\' (the line reports the tune it ran)')
     ap.add_argument("--peaks", action="store_true", help="print the measured ceilings only")
     ap.add_argument("--table-bits", type=int, default=30, help="--peaks: gather table of 2^bits words")
     args = ap.parse_args()
@@ -413,6 +416,8 @@ def main():
     engine = w.get("engine", "refill")
     # the 17-card engines run with their own defaults (war_enumerate_held / war_enumerate_wide, tune NULL)
     tune = war_gpu._tune_for(n, mode == 1, 0, w["flags"]) if engine == "refill" else None
+    if args.tune and engine == "refill":
+        tune = war_gpu.override_tune(tune, json.loads(args.tune))
 
     floyd_ms = []
 
