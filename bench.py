@@ -39,9 +39,9 @@ sys.path.insert(0, PKG)
 # war_turn / batched_kernel, not from compiled code.
 K_OPS_PER_TURN = 30
 # DRAM bytes (read + write) per deal of the path-memo refill kernel at this line's configuration (all 13!
-# deals, 8 GiB table): one-pass ncu capture of both launches of a timed step, 700.8 GB read and 13.1 GB
-# written for 6,227,020,800 deals (112.5 + 2.1 B per deal); each random 8-byte lookup costs a DRAM line.
-MEMO_DRAM_BYTES_PER_DEAL = 114.6
+# deals, 16 GiB table): one-pass ncu capture of both launches of a timed step, 699.5 GB read and 11.4 GB
+# written for 6,227,020,800 deals (112.3 + 1.8 B per deal); each random 8-byte lookup costs a DRAM line.
+MEMO_DRAM_BYTES_PER_DEAL = 114.2
 # Turns of the reference's own schedule (Brent with the tortoise saved at powers of two from the first turn)
 # over all 13! deals, as counted by an instrumented copy of cpu/war.cpp; the plain kernel reproduces it
 # exactly (its `turns`).
