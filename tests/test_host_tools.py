@@ -84,3 +84,31 @@ def test_bench_counts_the_extra_units_the_library_plans():
         lo = rnd.randrange(total)
         hi = min(total, lo + rnd.choice([1, 50, 5000, 10 ** 6, 10 ** 9, total]))
         assert bench.deal_extra_units(lo, hi, m) == len(warlib.plan(warlib.make_job(n, lo=lo, hi=hi), m)[2])
+
+
+def test_bench_cpu_baseline_times_the_program_of_each_engine():
+    """The cpu_baseline of the 17-card workloads samples the workload's own slice with the oracle's restatement of
+    the program that engine replaces (gpu/war17.py for the held-out engine, gpu/war24.py for the 5-bit engine),
+    and the main workloads the restatement of cpu/war.cpp; the line names which."""
+    import sys
+    import os
+    sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    import bench
+    for wl, prog in (("held17", "gpu/war17.py"), ("wide17", "gpu/war24.py"), ("deals11", "cpu/war.cpp")):
+        line = bench.cpu_baseline(bench.WORKLOADS[wl], target_s=0.2)
+        assert line["kind"] == "port" and line["value"] > 0 and line["unit"] == "deals/s"
+        assert prog in line["sample"], (wl, line["sample"])
+
+
+def test_tune_override():
+    """war_gpu.py --tune and bench.py --tune: fields of the stored tune replaced, unknown fields refused."""
+    import pytest
+    import war_gpu
+    import warlib
+    base = warlib.make_tune(threads=256, block_m=6, window=32, defer=8, variant=31, memo_bits=31)
+    t = war_gpu.override_tune(base, {"variant": 3, "threads": "512"})
+    assert (t.variant, t.threads, t.block_m, t.window, t.defer, t.memo_bits) == (3, 512, 6, 32, 8, 31)
+    assert base.variant == 31                       # a copy: the stored tune is left as it was
+    assert war_gpu.override_tune(None, {"defer": 16}).defer == 16
+    with pytest.raises(ValueError):
+        war_gpu.override_tune(base, {"no_such_field": 1})
