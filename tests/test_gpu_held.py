@@ -43,6 +43,23 @@ def test_a12_a13_recorded(wl, golden):
         assert (r["done"], r["cyc"], r["maxfin"], r["hist"]) == (g["deals"], g["cyc"], g["longest"], g["hist"])
 
 
+def test_recorded_17_card_slices(wl, golden):
+    """The reference's recorded 17-card runs that take seconds here (gpu/war24.py, data/long_runs.txt:61-75): 1e9
+    deals from 10^14, the first 8,992,587,776 deals and the last 785,219,584, through the held-out engine's
+    default turn and through the plain branching turn (variant 3) on the middle slice."""
+    seen = set()
+    for e in golden["war24"]:
+        if e["n"] != 17 or e["hi"] - e["lo"] > 10 ** 10 or (e["lo"], e["hi"]) in seen:
+            continue
+        seen.add((e["lo"], e["hi"]))
+        r = wl.enumerate_held(wl.make_job(17, lo=e["lo"], hi=e["hi"]))
+        assert (r.done, r.cyc, r.maxfin, r.undetermined) == (e["deals"], e["cyc"], e["longest"], 0), e
+        if e["lo"] == 10 ** 14:
+            r3 = wl.enumerate_held(wl.make_job(17, lo=e["lo"], hi=e["hi"]), wl.make_tune(variant=3))
+            assert (r3.done, r3.cyc, r3.maxfin, r3.turns) == (r.done, r.cyc, r.maxfin, r.turns)
+    assert len(seen) == 3
+
+
 @pytest.mark.parametrize("n", [14, 15, 16, 17])
 def test_slices_against_oracle(wl, oracle, n):
     import math
