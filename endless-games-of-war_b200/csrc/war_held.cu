@@ -5,7 +5,8 @@
 // out of the packed piles.  The state is the holder's other cards wh (lh of them), the opponent's cards
 // wo (lo), and the depth p of card n-1 in the holder's full pile (0 = on top); lh + lo = n - 1, so
 // (wh, wo, lh, p) is the whole position and Brent compares exactly that (gpu/war17.py:62-71).  The game
-// ends when the opponent has no card.
+// ends when the opponent has no card.  The default turn (h_turn_packed_fma) keeps lh and p in one word
+// s = 4 lh + 256 p and leaves lo implied, so Brent compares (wh, wo, s).
 //
 // The kernel is the refill design of war_refill.cuh for this state: a persistent grid, one game per lane,
 // outcomes latched every turn and recorded every `defer` turns by the whole warp, work units of aligned
