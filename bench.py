@@ -200,7 +200,7 @@ def reference_arm(args, rank, ws):
     _oracle_sample_rate(w, min(per_step, 5.0), cores)                   # warm-up
     times, done_units = [], 0
     for s in range(args.steps):
-        v, slice_len = _oracle_sample_rate(w, per_step, cores, seed=s + 1)
+        v, slice_len, _ = _oracle_sample_rate(w, per_step, cores, seed=s + 1)
         times.append(slice_len * 64 / v)
         done_units += slice_len * 64
     port = done_units / sum(times)
@@ -225,7 +225,8 @@ def reference_arm(args, rank, ws):
 
 def _oracle_sample_rate(w, target_s, cores, seed=0):
     """Times the oracle's restatement of the reference algorithm on a strided sample of the workload's
-    rank space (64 slices spread evenly), sized by a short probe to take about target_s seconds."""
+    rank space (64 slices spread evenly), sized by a short probe to take about target_s seconds.  Returns
+    (ranks per second, ranks per slice, seconds the sample took)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
     n, mode = w["n"], w["mode"]
@@ -249,24 +250,28 @@ def _oracle_sample_rate(w, target_s, cores, seed=0):
                 oracle.enumerate_job(job, cores)
         return time.time() - t0
 
-    probe = 4096
+    # grow the probe until it runs long enough for the per-call overhead not to dominate its rate
+    probe, cap = 4096, max(4096, total // 64)
     dt = run(probe)
-    slice_len = max(probe, int(probe * target_s / max(dt, 1e-3)))
+    while dt < min(1.0, target_s / 4) and probe < cap:
+        probe = min(cap, probe * 4)
+        dt = run(probe)
+    slice_len = min(cap, max(probe, int(probe * target_s / max(dt, 1e-3))))
     dt = run(slice_len)
-    return slice_len * 64 / dt, slice_len
+    return slice_len * 64 / dt, slice_len, dt
 
 
 def cpu_baseline(w, target_s=12.0):
     """The oracle's restatement of the reference algorithm on a bounded strided sample (all host threads)."""
     cores = os.cpu_count() or 1
-    v, slice_len = _oracle_sample_rate(w, target_s, cores)
+    v, slice_len, dt = _oracle_sample_rate(w, target_s, cores)
     mode = w["mode"]
     what = {"held": "gpu/war17.py's", "wide": "gpu/war24.py's"}.get(w.get("engine"), "cpu/war.cpp's")
     return {"value": v, "unit": "positions/s" if mode else "deals/s", "cores": cores, "kind": "port",
             "sample": "64 strided slices of %d ranks of the %s, oracle/war_oracle.c (restatement of "
-                      "%s algorithm, OpenMP on all host threads), ~%.0f s" % (
+                      "%s algorithm, OpenMP on all host threads), %.1f s" % (
                           slice_len, "workload's slice" if "engine" in w else
-                          ("canonical-position space" if mode else "deal space"), what, target_s)}
+                          ("canonical-position space" if mode else "deal space"), what, dt)}
 
 
 def deal_extra_units(lo, hi, m):
