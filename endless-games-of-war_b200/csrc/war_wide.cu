@@ -141,7 +141,10 @@ __device__ __forceinline__ bool wide_heap_step(WEnum& E) {
     return true;
 }
 
-template <int RULE, int DET>
+// SVC (Brent only): W is a multiple of the service period, so an undecided game (which starts at a service and
+// plays `period` turns between services) reaches each tortoise checkpoint W, 3W, 7W, ... exactly at a service,
+// and the checkpoint is saved there instead of being tested after every turn.
+template <int RULE, int DET, bool SVC>
 __global__ void __launch_bounds__(1024) wide_kernel(const __grid_constant__ WideArgs a, DevAcc* __restrict__ acc) {
     extern __shared__ u32 sh[];
     u32* shh = sh;                    // cycle-length histogram (Brent)
@@ -234,10 +237,13 @@ __global__ void __launch_bounds__(1024) wide_kernel(const __grid_constant__ Wide
                 const u32 kk = en ? (u32)K_END : (cy ? (u32)K_CYC : (r1 > cap ? (u32)K_UND : (u32)K_NONE));
                 rounds = open ? r1 : rounds;
                 kind = open ? kk : kind;
-                if (open && kk == K_NONE && r1 == next) {   // Brent: tortoise saved at W, 3W, 7W, ...
+                if (!SVC && open && kk == K_NONE && r1 == next) {   // Brent: tortoise saved at W, 3W, 7W, ...
                     t0 = a0; t1 = a1; t2 = b0; t3 = b1; next = 2u * next + W;
                 }
             }
+        }
+        if (DET == DET_BRENT && SVC && kind == K_NONE && rounds == next) {   // the checkpoint, at the service
+            t0 = a0; t1 = a1; t2 = b0; t3 = b1; next = 2u * next + W;
         }
         // service: record every decided game, refill its lane
         const bool fin = active & (kind != K_NONE);
@@ -278,17 +284,24 @@ __global__ void __launch_bounds__(1024) wide_kernel(const __grid_constant__ Wide
 
 typedef void (*WideFn)(const WideArgs, DevAcc*);
 
-static WideFn wide_pick(int det, int rule) {
-    if (det == DET_FLOYD) return rule ? wide_kernel<1, DET_FLOYD> : wide_kernel<0, DET_FLOYD>;
-    if (det == DET_STREAK) return wide_kernel<0, DET_STREAK>;
-    return rule ? wide_kernel<1, DET_BRENT> : wide_kernel<0, DET_BRENT>;
+static WideFn wide_pick(int det, int rule, bool svc) {
+    if (det == DET_FLOYD) return rule ? wide_kernel<1, DET_FLOYD, false> : wide_kernel<0, DET_FLOYD, false>;
+    if (det == DET_STREAK) return wide_kernel<0, DET_STREAK, false>;
+    if (svc) return rule ? wide_kernel<1, DET_BRENT, true> : wide_kernel<0, DET_BRENT, true>;
+    return rule ? wide_kernel<1, DET_BRENT, false> : wide_kernel<0, DET_BRENT, false>;
+}
+
+// Brent's checkpoints fall on services when W is a multiple of the service period.
+static bool wide_svc(int W, int defer) {
+    const int period = defer > 4 ? (defer + 3) & ~3 : 4;
+    return W % period == 0;
 }
 
 static size_t wide_shmem(int hbins) { return sizeof(u32) * (size_t)(hbins + WAR_EBINS + 32); }
 
-static int wide_max_blocks(int det, int rule, int threads, int hbins) {
+static int wide_max_blocks(int det, int rule, bool svc, int threads, int hbins) {
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, wide_pick(det, rule), threads, wide_shmem(hbins)) !=
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, wide_pick(det, rule, svc), threads, wide_shmem(hbins)) !=
         cudaSuccess)
         return 0;
     return nb;
@@ -334,7 +347,8 @@ extern "C" int war_enumerate_wide(const war_job* job, const war_wide_cfg* cfg, w
     if (job->lo == job->hi) return WAR_OK;
     int st;
     if ((st = ensure_ready())) return st;
-    const int maxb = wide_max_blocks(c.det, job->rule, threads, hbins);
+    const bool svc = wide_svc(W, defer);
+    const int maxb = wide_max_blocks(c.det, job->rule, svc, threads, hbins);
     if (maxb < 1) return fail(WAR_EINVAL, "launch shape threads=%d does not fit an SM", threads);
     const int bps = c.blocks_per_sm ? std::min(c.blocks_per_sm, maxb) : maxb;
     std::lock_guard<std::mutex> lk(ctx().mu);
@@ -361,7 +375,7 @@ extern "C" int war_enumerate_wide(const war_job* job, const war_wide_cfg* cfg, w
     // each launch plays fewer than 2^32 - 2^24 games (32-bit per-lane counters)
     const u64 per_unit = a.fact[block_m];
     const u64 max_units = std::max<u64>(1, ((1ull << 32) - (1ull << 24)) / per_unit);
-    const WideFn fnp = wide_pick(c.det, job->rule);
+    const WideFn fnp = wide_pick(c.det, job->rule, svc);
     const size_t shmem = wide_shmem(hbins);
     u64 done_main = 0;
     bool extras_done = p.extra.empty();
